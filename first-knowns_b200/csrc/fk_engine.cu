@@ -1,0 +1,1103 @@
+// fk_engine.cu -- libfk: host-side engine construction, the batch
+// pipeline and the C ABI declared in include/fk.h.
+//
+// Build (sm_100a only):
+//   nvcc -gencode arch=compute_100a,code=sm_100a -O3 -lineinfo -std=c++17 \
+//        -Xcompiler -fPIC -shared -o libfk.so fk_engine.cu
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/fk.h"
+#include "fk_arith.cuh"
+#include "fk_classify.cuh"
+#include "fk_sieve.cuh"
+#include "fk_types.h"
+
+using namespace fk;
+
+static thread_local std::string g_err;
+
+static fk_status set_err(fk_status s, const std::string& m) {
+  g_err = m;
+  return s;
+}
+
+#define FK_CUDA(call)                                                       \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess)                                                  \
+      return set_err(FK_ERR_DEVICE, std::string(#call) + ": " +            \
+                                        cudaGetErrorString(e_));            \
+  } while (0)
+
+// ------------------------------------------------------------------ math ---
+static u64 mulmod64(u64 a, u64 b, u64 m) { return (u64)((u128)a * b % m); }
+static u64 powmod64(u64 a, u64 e, u64 m) {
+  u64 r = 1 % m;
+  a %= m;
+  while (e) {
+    if (e & 1) r = mulmod64(r, a, m);
+    a = mulmod64(a, a, m);
+    e >>= 1;
+  }
+  return r;
+}
+static u64 invmod(u64 a, u64 q) { return powmod64(a % q, q - 2, q); }
+
+// Square roots of a modulo the odd prime q (Tonelli-Shanks); empty when a
+// is a non-residue.
+static std::vector<u64> sqrt_mod(u64 a, u64 q) {
+  a %= q;
+  if (a == 0) return {0};
+  if (powmod64(a, (q - 1) / 2, q) != 1) return {};
+  u64 r;
+  if (q % 4 == 3) {
+    r = powmod64(a, (q + 1) / 4, q);
+  } else {
+    u64 s = 0, t = q - 1;
+    while (t % 2 == 0) { t /= 2; ++s; }
+    u64 z = 2;
+    while (powmod64(z, (q - 1) / 2, q) != q - 1) ++z;
+    u64 c = powmod64(z, t, q), x = powmod64(a, (t + 1) / 2, q);
+    u64 tt = powmod64(a, t, q), mm = s;
+    while (tt != 1) {
+      u64 i = 0, t2 = tt;
+      while (t2 != 1) { t2 = mulmod64(t2, t2, q); ++i; }
+      u64 b = c;
+      for (u64 k = 0; k + i + 1 < mm; ++k) b = mulmod64(b, b, q);
+      x = mulmod64(x, b, q);
+      c = mulmod64(b, b, q);
+      tt = mulmod64(tt, c, q);
+      mm = i;
+    }
+    r = x;
+  }
+  if (r == q - r) return {r};
+  return {std::min(r, q - r), std::max(r, q - r)};
+}
+
+static std::vector<u32> primes_below(u32 lim) {
+  std::vector<u32> out;
+  if (lim <= 2) return out;
+  std::vector<uint8_t> f(lim, 1);
+  f[0] = f[1] = 0;
+  for (u64 i = 2; i * i < lim; ++i)
+    if (f[i])
+      for (u64 j = i * i; j < lim; j += i) f[j] = 0;
+  for (u32 i = 2; i < lim; ++i)
+    if (f[i]) out.push_back(i);
+  return out;
+}
+
+static u128 u128_of(const uint64_t v[2]) {
+  return ((u128)v[1] << 64) | v[0];
+}
+
+static std::string u128_str(u128 x) {
+  if (x == 0) return "0";
+  std::string s;
+  while (x) { s.push_back('0' + (int)(x % 10)); x /= 10; }
+  std::reverse(s.begin(), s.end());
+  return s;
+}
+
+// ---------------------------------------------------------------- engine ---
+struct fk_engine {
+  fk_params p{};
+  u32 kind = 0, n = 0, q2 = 0, P0 = 0;
+  u128 d = 0;         // AP difference
+  u64 W = 1;          // Dickson wheel modulus
+  u64 M = 1;
+  std::vector<u32> wheel;
+  std::vector<u64> lanes;
+  std::vector<u32> sieve;     // pattern primes, then per-candidate primes
+  std::vector<std::vector<u32>> forb;  // forbidden residues of x mod q
+  double survival = 1.0;      // expected survival through every sieve prime
+  DevEngine dev{};
+  std::vector<void*> allocs;
+  u64 device_bytes = 0;
+  fk_batch* plain = nullptr;  // internal single-engine batch
+  std::vector<uint64_t> res_off;
+  std::vector<uint8_t> res_depth;
+};
+
+static u32 first_sieve_prime(const fk_engine* e) {
+  return e->sieve.empty() ? 0 : e->sieve[0];
+}
+
+// Forbidden residues of the line variable x modulo q, by engine kind.
+static std::vector<u32> forbidden(const fk_engine* e, u32 q) {
+  std::vector<u32> f;
+  if (e->kind == KIND_EULER) {
+    // euler_search.py:85-87: p with q | x^2 + x + p for some x < n
+    for (u64 x = 0; x < e->n; ++x) f.push_back((u32)((q - (x * x + x) % q) % q));
+  } else if (e->kind == KIND_DICKSON) {
+    // ladder_search.py:71-89: j with m*(W*j)^2 + 1 == 0 mod q, m = 1..n
+    if (e->W % q == 0) return f;
+    const u64 winv = invmod(e->W % q, q);
+    for (u64 m = 1; m <= e->n; ++m) {
+      if (m % q == 0) continue;
+      const u64 rhs = (q - invmod(m, q)) % q;
+      for (u64 r : sqrt_mod(rhs, q)) f.push_back((u32)mulmod64(r, winv, q));
+    }
+  } else {
+    // ap_search.py:99-106: p with q | p + j*d for some j < n; the mod-30
+    // wheel primes kill only multiples of themselves (ap_search.py:91-93)
+    if (q == 2 || q == 3 || q == 5) return {0};
+    const u64 dq = (u64)(e->d % q);
+    for (u64 j = 0; j < e->n; ++j) f.push_back((u32)((q - (j * dq) % q) % q));
+  }
+  std::sort(f.begin(), f.end());
+  f.erase(std::unique(f.begin(), f.end()), f.end());
+  return f;
+}
+
+static bool is_sieve_prime(const fk_engine* e, u32 q) {
+  if (e->kind == KIND_DICKSON) return q >= e->n + 2;
+  return true;
+}
+
+template <typename T, typename D>
+static fk_status upload(fk_engine* e, const std::vector<T>& h, const D** dptr,
+                        size_t min_bytes = 0) {
+  static_assert(sizeof(T) == sizeof(D), "element size mismatch");
+  size_t bytes = std::max(h.size() * sizeof(T), min_bytes);
+  bytes = std::max<size_t>(bytes, 16);
+  void* p = nullptr;
+  FK_CUDA(cudaMalloc(&p, bytes));
+  e->allocs.push_back(p);
+  e->device_bytes += bytes;
+  FK_CUDA(cudaMemset(p, 0, bytes));
+  if (!h.empty()) FK_CUDA(cudaMemcpy(p, h.data(), h.size() * sizeof(T),
+                                     cudaMemcpyHostToDevice));
+  *dptr = (const D*)p;
+  return FK_OK;
+}
+
+static u32 pat_bytes_for(u32 P0) {
+  switch (P0) {
+    case 3: return pat_bytes<3>();
+    case 6: return pat_bytes<6>();
+    case 9: return pat_bytes<9>();
+    default: return pat_bytes<12>();
+  }
+}
+
+static fk_status build_engine(fk_engine* e) {
+  const fk_params& p = e->p;
+  e->kind = p.kind;
+  e->n = p.n;
+  e->q2 = p.q2 ? p.q2 : 65536;
+  if (e->kind > KIND_AP) return set_err(FK_ERR_DOMAIN, "unknown engine kind");
+  if (e->n < 1 || e->n > 60)
+    return set_err(FK_ERR_DOMAIN, "n must be in [1, 60]");
+  if (e->q2 > (1u << 30))
+    return set_err(FK_ERR_DOMAIN, "q2 must be at most 2^30 (Barrett range)");
+  u32 P0 = p.p0;
+  if (P0 == 0) P0 = (e->kind == KIND_EULER) ? 6 : (e->kind == KIND_AP ? 6 : 6);
+  if (P0 != 3 && P0 != 6 && P0 != 9 && P0 != 12)
+    return set_err(FK_ERR_DOMAIN, "p0 must be 3, 6, 9 or 12");
+  e->P0 = P0;
+  const u32 first_pat = fk_nth_prime((int)P0);
+  const u32 last_pat = fk_nth_prime((int)P0 + kNS - 1);
+  if (e->q2 <= last_pat + 1)
+    return set_err(FK_ERR_DOMAIN, "q2 " + std::to_string(e->q2) +
+                                      " is too small for the pattern sieve "
+                                      "(needs > " + std::to_string(last_pat + 1) + ")");
+  if (e->kind == KIND_DICKSON) {
+    // ladder_reference.py:60-66: W = product of primes <= n + 1
+    u64 w = 1;
+    for (u32 q : primes_below(e->n + 2)) w *= q;
+    e->W = w;
+  }
+  if (e->kind == KIND_AP) {
+    u128 d = ((u128)p.d_hi << 64) | p.d_lo;
+    if (d == 0) {
+      // ap_reference.py:99-110: the n-th primorial
+      d = 1;
+      auto pr = primes_below(1000);
+      for (u32 i = 0; i < e->n; ++i) d *= pr[i];
+    }
+    e->d = d;
+  }
+  const std::vector<u32> all = primes_below(e->q2);
+  // wheel: sieve primes below the first pattern prime, folded into lanes
+  e->lanes.assign(1, 0);
+  e->M = 1;
+  e->wheel.clear();
+  for (u32 q : all) {
+    if (q >= first_pat) break;
+    if (!is_sieve_prime(e, q)) continue;
+    std::vector<u32> f = forbidden(e, q);
+    if (f.empty()) continue;
+    std::vector<uint8_t> bad(q, 0);
+    for (u32 r : f) bad[r] = 1;
+    std::vector<u64> nl;
+    const u64 cnt = (u64)e->lanes.size() * (q - f.size());
+    if (cnt > (1ull << 22))
+      return set_err(FK_ERR_DOMAIN, "wheel has too many lanes; use a smaller p0");
+    nl.reserve(cnt);
+    for (u64 t = 0; t < q; ++t)
+      for (u64 r : e->lanes) {
+        const u64 x = r + t * e->M;
+        if (!bad[x % q]) nl.push_back(x);
+      }
+    std::sort(nl.begin(), nl.end());
+    e->lanes.swap(nl);
+    e->M *= q;
+    e->wheel.push_back(q);
+    e->survival *= 1.0 - (double)f.size() / q;
+  }
+  if (e->lanes.empty())
+    return set_err(FK_ERR_DOMAIN, "the wheel admits no residue: no survivors exist");
+  // sieve primes from the first pattern prime up
+  e->sieve.clear();
+  e->forb.clear();
+  for (u32 q : all) {
+    if (q < first_pat) continue;
+    e->sieve.push_back(q);
+    e->forb.push_back(is_sieve_prime(e, q) ? forbidden(e, q) : std::vector<u32>());
+  }
+  const u32 NP = (u32)e->sieve.size();
+  // ---- pattern tables (the first kNS sieve primes) -----------------------
+  std::vector<u64> pat;
+  std::vector<u32> minv(kNS);
+  for (int i = 0; i < kNS; ++i) {
+    const u32 q = e->sieve[i];
+    if (q != fk_nth_prime((int)P0 + i))
+      return set_err(FK_ERR_DEVICE, "pattern prime layout mismatch");
+    const u64 mq = e->M % q;
+    const u64 mi = invmod(mq, q);
+    minv[i] = (u32)mi;
+    std::vector<uint8_t> g(q, 0);
+    for (u32 f : e->forb[i]) g[mulmod64(f, mi, q)] = 1;
+    for (u32 rho = 0; rho < q; ++rho) {
+      u64 w = 0;
+      for (u32 b = 0; b < 64; ++b)
+        if (g[(rho + b) % q]) w |= 1ull << b;
+      pat.push_back(w);
+    }
+    e->survival *= 1.0 - (double)e->forb[i].size() / q;
+  }
+  // ---- per-candidate primes -----------------------------------------------
+  u32 xxmax = 0;
+  std::vector<u32> sbits;
+  if (e->kind == KIND_EULER) {
+    xxmax = (e->n - 1) * (e->n - 1) + (e->n - 1);
+    sbits.assign(xxmax / 32 + 1, 0);
+    for (u32 x = 0; x < e->n; ++x) {
+      const u32 v = x * x + x;
+      sbits[v >> 5] |= 1u << (v & 31);
+    }
+    if (sbits.size() > 512)
+      return set_err(FK_ERR_DOMAIN, "n too large for the Euler bitset test");
+  }
+  std::vector<PrimeRec> recs(NP);
+  std::vector<u32> c64(NP), lists;
+  for (u32 i = 0; i < NP; ++i) {
+    const u32 q = e->sieve[i];
+    PrimeRec r;
+    r.q = q;
+    r.magic = (u64)(((u128)1 << 64) / q);
+    r.aux = 0;
+    c64[i] = (u32)(((u128)1 << 64) % q);
+    const auto& f = e->forb[i];
+    bool use_list = false;
+    if (e->kind == KIND_DICKSON) use_list = true;
+    if (e->kind == KIND_EULER && q <= xxmax) use_list = true;
+    if (e->kind == KIND_AP) {
+      const u64 dq = (u64)(e->d % q);
+      r.aux = dq ? (u32)invmod(dq, q) : 0;
+    }
+    if (use_list && i >= (u32)kNS) {
+      if (f.size() > 127) return set_err(FK_ERR_DOMAIN, "forbidden list too long");
+      if (lists.size() >= (1u << 24)) return set_err(FK_ERR_DOMAIN, "lists too large");
+      r.aux = 0x80000000u | ((u32)f.size() << 24) | (u32)lists.size();
+      lists.insert(lists.end(), f.begin(), f.end());
+    }
+    recs[i] = r;
+  }
+  // ---- compaction rounds: a round ends when survival within it halves ----
+  std::vector<u32> rounds;
+  rounds.push_back(kNS);
+  double s = 1.0;
+  u32 start = kNS;
+  for (u32 i = kNS; i < NP; ++i) {
+    s *= 1.0 - (double)e->forb[i].size() / e->sieve[i];
+    e->survival *= 1.0 - (double)e->forb[i].size() / e->sieve[i];
+    if ((s < 0.5 || i + 1 - start >= 4096) && i + 1 < NP) {
+      rounds.push_back(i + 1);
+      s = 1.0;
+      start = i + 1;
+    }
+  }
+  rounds.push_back(NP);
+  if (rounds.size() > (size_t)kMaxRounds + 1) {
+    rounds.resize(kMaxRounds);
+    rounds.push_back(NP);
+  }
+  if (NP <= (u32)kNS) rounds.assign({(u32)kNS, (u32)kNS});
+  // ---- upload -------------------------------------------------------------
+  DevEngine& d = e->dev;
+  d.kind = e->kind;
+  d.n = e->n;
+  d.L = (u32)e->lanes.size();
+  d.NP = NP;
+  d.P0 = P0;
+  d.NS = kNS;
+  d.nrounds = (u32)rounds.size() - 1;
+  d.xxmax = xxmax;
+  d.pat_words = (u32)pat.size();
+  d.sbits_words = (u32)sbits.size();
+  d.two_pass = p.two_pass;
+  d.M = e->M;
+  d.W = e->W;
+  d.d_lo = (u64)e->d;
+  d.d_hi = (u64)(e->d >> 64);
+  fk_status st;
+  if ((st = upload(e, e->lanes, &d.lanes))) return st;
+  if ((st = upload(e, pat, &d.pat, pat_bytes_for(P0)))) return st;
+  if ((st = upload(e, minv, &d.pat_minv))) return st;
+  if ((st = upload(e, recs, &d.recs))) return st;
+  if ((st = upload(e, c64, &d.c64))) return st;
+  if ((st = upload(e, lists, &d.lists))) return st;
+  if ((st = upload(e, rounds, &d.rounds))) return st;
+  if ((st = upload(e, sbits, &d.sbits))) return st;
+  return FK_OK;
+}
+
+// ----------------------------------------------------------------- batch ---
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  u64 cap = 0;
+  fk_status ensure(u64 n) {
+    if (n <= cap && p) return FK_OK;
+    u64 c = std::max<u64>(n, 1024);
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    FK_CUDA(cudaMalloc(&p, c * sizeof(T)));
+    cap = c;
+    return FK_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+template <typename T>
+struct PinBuf {
+  T* p = nullptr;
+  u64 cap = 0;
+  fk_status ensure(u64 n) {
+    if (n <= cap && p) return FK_OK;
+    u64 c = std::max<u64>(n, 1024);
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    FK_CUDA(cudaMallocHost(&p, c * sizeof(T)));
+    cap = c;
+    return FK_OK;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+struct SubItem {
+  u32 user;       // index of the user item
+  u128 X0;        // line base
+};
+
+struct Family {
+  u32 P0;
+  std::vector<u32> idx;         // internal item indices
+  std::vector<u64> prefix;      // task prefix, size idx+1
+  DevBuf<u32> d_idx;
+  DevBuf<u64> d_prefix;
+};
+
+struct fk_batch {
+  std::vector<fk_engine*> engines;
+  DevEngine* d_engines = nullptr;
+  cudaStream_t stream = nullptr;
+  int nsm = 148;
+  // host-side item expansion
+  std::vector<fk_item> user;
+  std::vector<DevItem> items;
+  std::vector<SubItem> sub;
+  std::vector<u32> dense_idx, sieve_idx;
+  Family fam[4];
+  // device buffers
+  DevBuf<DevItem> d_items;
+  DevBuf<u32> d_dense, d_sieve;
+  DevBuf<u32> d_xq;
+  DevBuf<u64> d_cand_key;
+  DevBuf<u32> d_cand_item;
+  DevBuf<OutRec> d_out;
+  DevBuf<u32> d_item_count, d_item_fill;
+  DevBuf<u64> d_item_off, d_sorted, d_scratch;
+  DevBuf<unsigned long long> d_task_ctr;
+  DevBuf<u32> d_nitems;
+  DevCounters* d_ctr = nullptr;
+  PinBuf<DevItem> h_items;
+  PinBuf<DevCounters> h_ctr;
+  PinBuf<u64> h_off, h_sorted;
+  PinBuf<u32> h_small;
+  PinBuf<u64> h_prefix;
+  u64 cand_cap = 0, out_cap = 0;
+  // graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<u64> graph_key;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // results
+  std::vector<uint64_t> r_start, r_off;
+  std::vector<uint8_t> r_depth;
+  bool pending = false;
+  int pending_graph = 0;
+};
+
+static const int kOccupancy = 2;
+
+static fk_status batch_init(fk_batch* b, fk_engine* const* engines,
+                            u32 nengines) {
+  b->engines.assign(engines, engines + nengines);
+  std::vector<DevEngine> de(nengines);
+  for (u32 i = 0; i < nengines; ++i) de[i] = engines[i]->dev;
+  FK_CUDA(cudaMalloc(&b->d_engines, sizeof(DevEngine) * std::max<u32>(nengines, 1)));
+  FK_CUDA(cudaMemcpy(b->d_engines, de.data(), sizeof(DevEngine) * nengines,
+                     cudaMemcpyHostToDevice));
+  FK_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  FK_CUDA(cudaMalloc(&b->d_ctr, sizeof(DevCounters)));
+  int dev = 0;
+  FK_CUDA(cudaGetDevice(&dev));
+  FK_CUDA(cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, dev));
+  for (int i = 0; i < 4; ++i) FK_CUDA(cudaEventCreate(&b->ev[i]));
+  const u32 P0s[4] = {3, 6, 9, 12};
+  for (int f = 0; f < 4; ++f) b->fam[f].P0 = P0s[f];
+  FK_CUDA(b->d_task_ctr.ensure(4) == FK_OK ? cudaSuccess : cudaErrorMemoryAllocation);
+  FK_CUDA(b->d_nitems.ensure(4) == FK_OK ? cudaSuccess : cudaErrorMemoryAllocation);
+  FK_CUDA(b->h_ctr.ensure(1) == FK_OK ? cudaSuccess : cudaErrorMemoryAllocation);
+  static bool attrs_done = false;
+  if (!attrs_done) {
+    FK_CUDA(cudaFuncSetAttribute(k_sieve<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(pat_bytes<3>() + sizeof(SieveSmem))));
+    FK_CUDA(cudaFuncSetAttribute(k_sieve<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(pat_bytes<6>() + sizeof(SieveSmem))));
+    FK_CUDA(cudaFuncSetAttribute(k_sieve<9>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(pat_bytes<9>() + sizeof(SieveSmem))));
+    FK_CUDA(cudaFuncSetAttribute(k_sieve<12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(pat_bytes<12>() + sizeof(SieveSmem))));
+    attrs_done = true;
+  }
+  return FK_OK;
+}
+
+static void batch_free(fk_batch* b) {
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->d_items.release(); b->d_dense.release(); b->d_sieve.release();
+  b->d_xq.release(); b->d_cand_key.release(); b->d_cand_item.release();
+  b->d_out.release(); b->d_item_count.release(); b->d_item_fill.release();
+  b->d_item_off.release(); b->d_sorted.release(); b->d_scratch.release();
+  b->d_task_ctr.release(); b->d_nitems.release();
+  for (auto& f : b->fam) { f.d_idx.release(); f.d_prefix.release(); }
+  b->h_items.release(); b->h_ctr.release(); b->h_off.release();
+  b->h_sorted.release(); b->h_small.release(); b->h_prefix.release();
+  if (b->d_ctr) cudaFree(b->d_ctr);
+  if (b->d_engines) cudaFree(b->d_engines);
+  for (auto& e : b->ev) if (e) cudaEventDestroy(e);
+  if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+static int fam_of(u32 P0) { return P0 == 3 ? 0 : P0 == 6 ? 1 : P0 == 9 ? 2 : 3; }
+
+// Largest value a chain can produce must fit three limbs.
+static bool chain_fits(const fk_engine* e, u128 x_hi, u32 cap, bool dense) {
+  const long double lim = std::ldexp(1.0L, 190);
+  const long double x = (long double)x_hi;
+  if (e->kind == KIND_EULER) return x + (long double)cap * cap + cap < std::ldexp(1.0L, 127);
+  if (e->kind == KIND_DICKSON) {
+    const long double k = x * (dense ? 1.0L : (long double)e->W);
+    return k < std::ldexp(1.0L, 126) && (long double)(cap + 1) * k * k < lim;
+  }
+  return x < std::ldexp(1.0L, 127) && x + (long double)cap * (long double)e->d < lim;
+}
+
+// Expand user items into device items (launch-sized sub-ranges).
+static fk_status expand(fk_batch* b, const fk_item* items, u64 nitems) {
+  b->user.assign(items, items + nitems);
+  b->items.clear();
+  b->sub.clear();
+  b->dense_idx.clear();
+  b->sieve_idx.clear();
+  for (auto& f : b->fam) { f.idx.clear(); f.prefix.assign(1, 0); }
+  const u64 target_chains = (u64)b->nsm * kOccupancy * kBlock * 4;
+  for (u64 ui = 0; ui < nitems; ++ui) {
+    const fk_item& it = items[ui];
+    if (it.engine >= b->engines.size())
+      return set_err(FK_ERR_ARG, "item engine index out of range");
+    const fk_engine* e = b->engines[it.engine];
+    const u128 lo = u128_of(it.lo), hi = u128_of(it.hi);
+    if (hi <= lo) continue;
+    if (hi - lo >= ((u128)1 << 63))
+      return set_err(FK_ERR_DOMAIN, "interval wider than 2^63");
+    if (it.mode > MODE_DENSE) return set_err(FK_ERR_ARG, "bad mode");
+    if (it.cap > 250) return set_err(FK_ERR_DOMAIN, "cap above 250");
+    if (!chain_fits(e, hi, std::max(it.cap, it.threshold), it.mode == MODE_DENSE))
+      return set_err(FK_ERR_DOMAIN, "values past 190 bits at " + u128_str(hi));
+    if (it.mode == MODE_DENSE) {
+      const u64 cnt = (u64)(hi - lo);
+      if (cnt > (1ull << 26)) return set_err(FK_ERR_DOMAIN, "dense range above 2^26");
+      DevItem di{};
+      di.engine = it.engine;
+      di.mode = MODE_DENSE;
+      di.threshold = it.threshold;
+      di.cap = it.cap;
+      di.X0_lo = (u64)lo;
+      di.X0_hi = (u64)(lo >> 64);
+      di.U = cnt;
+      b->dense_idx.push_back((u32)b->items.size());
+      b->items.push_back(di);
+      b->sub.push_back({(u32)ui, lo});
+      continue;
+    }
+    const u64 M = e->M;
+    const u128 X0 = lo / M * M;
+    const u128 periods = (hi - X0 + M - 1) / M;
+    // periods per device item: offsets u*M + R stay below 2^55
+    u64 umax = (u64)(((u128)1 << 55) / M);
+    umax = std::max<u64>(64, umax / 64 * 64);
+    umax = std::min<u64>(umax, 1ull << 36);
+    const u64 L = e->lanes.size();
+    for (u128 s0 = 0; s0 < periods; s0 += umax) {
+      const u64 U = (u64)std::min<u128>(umax, periods - s0);
+      DevItem di{};
+      di.engine = it.engine;
+      di.mode = it.mode;
+      di.threshold = it.threshold;
+      di.cap = it.cap;
+      const u128 base = X0 + s0 * M;
+      di.X0_lo = (u64)base;
+      di.X0_hi = (u64)(base >> 64);
+      di.U = U;
+      di.lo_off = (s0 == 0) ? (u64)(lo - X0) : 0;
+      const bool last = s0 + U >= periods;
+      di.hi_last = last ? (u64)(hi - (base + (u128)(U - 1) * M)) : M;
+      const u64 words = (U + 63) / 64;
+      u64 tc = (words * L + target_chains - 1) / target_chains;
+      tc = std::min<u64>(std::max<u64>(tc, 1), 256);
+      di.Tc = (u32)tc;
+      di.nchunk = (words + tc - 1) / tc;
+      const u64 chains = di.nchunk * L;
+      di.ntask = (chains + kBlock - 1) / kBlock;
+      Family& f = b->fam[fam_of(e->P0)];
+      di.task0 = f.prefix.back();
+      f.prefix.push_back(f.prefix.back() + di.ntask);
+      f.idx.push_back((u32)b->items.size());
+      b->sieve_idx.push_back((u32)b->items.size());
+      b->items.push_back(di);
+      b->sub.push_back({(u32)ui, base});
+    }
+  }
+  // base-residue table offsets
+  u64 xo = 0;
+  for (u32 i : b->sieve_idx) {
+    b->items[i].xq_off = xo;
+    xo += b->engines[b->items[i].engine]->sieve.size();
+  }
+  if (xo >= (1ull << 32) * 4) return set_err(FK_ERR_DOMAIN, "batch too large");
+  fk_status st;
+  if ((st = b->d_xq.ensure(xo + 16))) return st;
+  // capacities from the survival model
+  long double expect = 0;
+  for (size_t i = 0; i < b->items.size(); ++i) {
+    const DevItem& di = b->items[i];
+    if (di.mode == MODE_DENSE) { expect += di.U; continue; }
+    const fk_engine* e = b->engines[di.engine];
+    expect += (long double)di.U * e->lanes.size() * e->survival * 3.0L + 64;
+  }
+  const u64 need = (u64)std::min<long double>(expect * 2 + 4096, (long double)(1ull << 28));
+  if (need > b->cand_cap) {
+    if ((st = b->d_cand_key.ensure(need))) return st;
+    if ((st = b->d_cand_item.ensure(need))) return st;
+    b->cand_cap = need;
+  }
+  if (need > b->out_cap) {
+    if ((st = b->d_out.ensure(need))) return st;
+    if ((st = b->d_sorted.ensure(need))) return st;
+    if ((st = b->d_scratch.ensure(2 * need))) return st;
+    b->out_cap = need;
+  }
+  const u64 ni = b->items.size();
+  if ((st = b->d_items.ensure(ni + 1))) return st;
+  if ((st = b->d_item_count.ensure(ni + 1))) return st;
+  if ((st = b->d_item_fill.ensure(ni + 1))) return st;
+  if ((st = b->d_item_off.ensure(ni + 2))) return st;
+  if ((st = b->h_items.ensure(ni + 1))) return st;
+  if ((st = b->h_off.ensure(ni + 2))) return st;
+  if ((st = b->d_dense.ensure(b->dense_idx.size() + 1))) return st;
+  if ((st = b->d_sieve.ensure(b->sieve_idx.size() + 1))) return st;
+  u64 famsz = 0, fampre = 0;
+  for (auto& f : b->fam) { famsz += f.idx.size(); fampre += f.prefix.size(); }
+  if ((st = b->h_small.ensure(b->dense_idx.size() + b->sieve_idx.size() + famsz + 8))) return st;
+  if ((st = b->h_prefix.ensure(fampre + 8))) return st;
+  for (auto& f : b->fam) {
+    if ((st = f.d_idx.ensure(f.idx.size() + 1))) return st;
+    if ((st = f.d_prefix.ensure(f.prefix.size() + 1))) return st;
+  }
+  return FK_OK;
+}
+
+// Enqueue the whole pipeline on the batch stream (graph-capturable: no
+// host synchronisation, every size it needs is already on the device).
+static fk_status enqueue(fk_batch* b) {
+  cudaStream_t s = b->stream;
+  const u32 ni = (u32)b->items.size();
+  FK_CUDA(cudaMemsetAsync(b->d_ctr, 0, sizeof(DevCounters), s));
+  FK_CUDA(cudaMemsetAsync(b->d_task_ctr.p, 0, 4 * sizeof(unsigned long long), s));
+  FK_CUDA(cudaMemsetAsync(b->d_item_count.p, 0, (ni + 1) * sizeof(u32), s));
+  FK_CUDA(cudaMemsetAsync(b->d_item_fill.p, 0, (ni + 1) * sizeof(u32), s));
+  FK_CUDA(cudaEventRecord(b->ev[0], s));
+  if (!b->sieve_idx.empty()) {
+    dim3 g(64, (u32)std::min<size_t>(b->sieve_idx.size(), 65535));
+    k_xq<<<g, kBlock, 0, s>>>(b->d_engines, b->d_items.p, b->d_sieve.p,
+                              (u32)b->sieve_idx.size(), b->d_xq.p);
+  }
+  if (!b->dense_idx.empty()) {
+    k_dense<<<b->nsm * 4, kBlock, 0, s>>>(b->d_items.p, b->d_dense.p,
+                                          (u32)b->dense_idx.size(),
+                                          b->d_cand_key.p, b->d_cand_item.p,
+                                          b->cand_cap, b->d_ctr);
+  }
+  for (int f = 0; f < 4; ++f) {
+    Family& F = b->fam[f];
+    if (F.idx.empty()) continue;
+    SieveArgs a{};
+    a.engines = b->d_engines;
+    a.items = b->d_items.p;
+    a.task_prefix = F.d_prefix.p;
+    a.item_index = F.d_idx.p;
+    a.nitems = (u32)F.idx.size();
+    a.ntask = F.prefix.back();
+    a.xq = b->d_xq.p;
+    a.cand_key = b->d_cand_key.p;
+    a.cand_item = b->d_cand_item.p;
+    a.cand_cap = b->cand_cap;
+    a.ctr = b->d_ctr;
+    a.task_ctr = b->d_task_ctr.p + f;
+    const u64 grid = std::min<u64>(a.ntask, (u64)b->nsm * kOccupancy);
+    const u32 P0 = F.P0;
+    const size_t sm = pat_bytes_for(P0) + sizeof(SieveSmem);
+    switch (P0) {
+      case 3: k_sieve<3><<<(u32)grid, kBlock, sm, s>>>(a); break;
+      case 6: k_sieve<6><<<(u32)grid, kBlock, sm, s>>>(a); break;
+      case 9: k_sieve<9><<<(u32)grid, kBlock, sm, s>>>(a); break;
+      default: k_sieve<12><<<(u32)grid, kBlock, sm, s>>>(a); break;
+    }
+  }
+  FK_CUDA(cudaGetLastError());
+  FK_CUDA(cudaEventRecord(b->ev[1], s));
+  ClassArgs c{};
+  c.engines = b->d_engines;
+  c.items = b->d_items.p;
+  c.cand_key = b->d_cand_key.p;
+  c.cand_item = b->d_cand_item.p;
+  c.cand_cap = b->cand_cap;
+  c.ctr = b->d_ctr;
+  c.out = b->d_out.p;
+  c.out_cap = b->out_cap;
+  c.item_count = b->d_item_count.p;
+  k_classify<<<b->nsm * 8, kBlock, 0, s>>>(c);
+  FK_CUDA(cudaEventRecord(b->ev[2], s));
+  k_scan<<<1, kBlock, 0, s>>>(b->d_item_count.p, ni, b->d_item_off.p);
+  k_scatter<<<b->nsm * 2, kBlock, 0, s>>>(b->d_out.p, b->d_ctr, b->out_cap,
+                                          b->d_item_off.p, b->d_item_fill.p,
+                                          b->d_sorted.p);
+  k_sort_seg<<<(u32)std::min<u64>(std::max<u32>(ni, 1), (u64)b->nsm * 4), kBlock, 0, s>>>(
+      b->d_sorted.p, b->d_item_off.p, b->d_nitems.p, b->d_scratch.p);
+  FK_CUDA(cudaGetLastError());
+  FK_CUDA(cudaEventRecord(b->ev[3], s));
+  FK_CUDA(cudaMemcpyAsync(b->h_ctr.p, b->d_ctr, sizeof(DevCounters),
+                          cudaMemcpyDeviceToHost, s));
+  FK_CUDA(cudaMemcpyAsync(b->h_off.p, b->d_item_off.p, (ni + 1) * sizeof(u64),
+                          cudaMemcpyDeviceToHost, s));
+  return FK_OK;
+}
+
+static fk_status upload_items(fk_batch* b) {
+  cudaStream_t s = b->stream;
+  const u64 ni = b->items.size();
+  std::copy(b->items.begin(), b->items.end(), b->h_items.p);
+  FK_CUDA(cudaMemcpyAsync(b->d_items.p, b->h_items.p, ni * sizeof(DevItem),
+                          cudaMemcpyHostToDevice, s));
+  u32* hs = b->h_small.p;
+  size_t k = 0;
+  for (u32 v : b->dense_idx) hs[k++] = v;
+  for (u32 v : b->sieve_idx) hs[k++] = v;
+  hs[k] = (u32)ni;
+  if (!b->dense_idx.empty())
+    FK_CUDA(cudaMemcpyAsync(b->d_dense.p, hs, b->dense_idx.size() * 4,
+                            cudaMemcpyHostToDevice, s));
+  if (!b->sieve_idx.empty())
+    FK_CUDA(cudaMemcpyAsync(b->d_sieve.p, hs + b->dense_idx.size(),
+                            b->sieve_idx.size() * 4, cudaMemcpyHostToDevice, s));
+  FK_CUDA(cudaMemcpyAsync(b->d_nitems.p, hs + k, 4, cudaMemcpyHostToDevice, s));
+  ++k;
+  u64* hp = b->h_prefix.p;
+  size_t kp = 0;
+  for (auto& f : b->fam) {
+    if (f.idx.empty()) continue;
+    std::copy(f.idx.begin(), f.idx.end(), hs + k);
+    FK_CUDA(cudaMemcpyAsync(f.d_idx.p, hs + k, f.idx.size() * 4,
+                            cudaMemcpyHostToDevice, s));
+    k += f.idx.size();
+    std::copy(f.prefix.begin(), f.prefix.end(), hp + kp);
+    FK_CUDA(cudaMemcpyAsync(f.d_prefix.p, hp + kp, f.prefix.size() * 8,
+                            cudaMemcpyHostToDevice, s));
+    kp += f.prefix.size();
+  }
+  return FK_OK;
+}
+
+static fk_status launch(fk_batch* b, int use_graph) {
+  if (!use_graph) return enqueue(b);
+  std::vector<u64> key;
+  key.push_back(b->items.size());
+  key.push_back(b->dense_idx.size());
+  key.push_back(b->sieve_idx.size());
+  key.push_back(b->cand_cap);
+  key.push_back(b->out_cap);
+  key.push_back(b->d_xq.cap);
+  for (auto& f : b->fam) { key.push_back(f.idx.size()); key.push_back(f.prefix.back()); }
+  key.push_back((u64)(uintptr_t)b->d_items.p);
+  key.push_back((u64)(uintptr_t)b->d_cand_key.p);
+  if (b->gexec == nullptr || key != b->graph_key) {
+    if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    FK_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    fk_status st = enqueue(b);
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+    if (st) { if (g) cudaGraphDestroy(g); return st; }
+    if (ce != cudaSuccess) return set_err(FK_ERR_DEVICE, cudaGetErrorString(ce));
+    b->graph = g;
+    FK_CUDA(cudaGraphInstantiate(&b->gexec, g, 0));
+    b->graph_key = key;
+  }
+  FK_CUDA(cudaGraphLaunch(b->gexec, b->stream));
+  return FK_OK;
+}
+
+// Wait for a launched run, read the ordered stream back and unpack it per
+// user item.  Returns FK_ERR_OVERFLOW (with the buffers grown) when a
+// capacity was exceeded; the caller reruns.
+static fk_status collect(fk_batch* b) {
+  cudaStream_t s = b->stream;
+  FK_CUDA(cudaStreamSynchronize(s));
+  const DevCounters c = *b->h_ctr.p;
+  if (c.overflow & 4u)
+    return set_err(FK_ERR_TIMEOUT, "a bounded device wait gave up (pattern staging)");
+  if (c.overflow & 8u)
+    return set_err(FK_ERR_DOMAIN, "a chain value exceeded 192 bits");
+  if (c.overflow & 3u) {
+    const u64 need = std::max<u64>({c.ncand, c.nout, b->cand_cap}) * 2 + 4096;
+    fk_status st;
+    if ((st = b->d_cand_key.ensure(need))) return st;
+    if ((st = b->d_cand_item.ensure(need))) return st;
+    if ((st = b->d_out.ensure(need))) return st;
+    if ((st = b->d_sorted.ensure(need))) return st;
+    if ((st = b->d_scratch.ensure(2 * need))) return st;
+    b->cand_cap = b->out_cap = need;
+    return set_err(FK_ERR_OVERFLOW, "candidate buffer overflow (grown; rerun)");
+  }
+  const u64 ni = b->items.size();
+  const u64 nout = b->h_off.p[ni];
+  fk_status st;
+  if ((st = b->h_sorted.ensure(nout + 1))) return st;
+  if (nout) {
+    FK_CUDA(cudaMemcpyAsync(b->h_sorted.p, b->d_sorted.p, nout * 8,
+                            cudaMemcpyDeviceToHost, s));
+    FK_CUDA(cudaStreamSynchronize(s));
+  }
+  const u64 nu = b->user.size();
+  b->r_start.assign(nu + 1, 0);
+  b->r_off.resize(nout);
+  b->r_depth.resize(nout);
+  // internal items are in user order, and within a user item ascending
+  std::vector<u64> cnt(nu, 0);
+  for (u64 i = 0; i < ni; ++i) cnt[b->sub[i].user] += b->h_off.p[i + 1] - b->h_off.p[i];
+  for (u64 u = 0; u < nu; ++u) b->r_start[u + 1] = b->r_start[u] + cnt[u];
+  std::vector<u64> fill(b->r_start.begin(), b->r_start.end() - 1);
+  for (u64 i = 0; i < ni; ++i) {
+    const u32 u = b->sub[i].user;
+    const u128 lo = u128_of(b->user[u].lo);
+    const u64 base = (u64)(b->sub[i].X0 - lo);  // X0 >= lo - M ... may wrap
+    for (u64 k = b->h_off.p[i]; k < b->h_off.p[i + 1]; ++k) {
+      const u64 pk = b->h_sorted.p[k];
+      b->r_off[fill[u]] = base + (pk >> 8);
+      b->r_depth[fill[u]] = (uint8_t)(pk & 255);
+      ++fill[u];
+    }
+  }
+  return FK_OK;
+}
+
+static fk_status batch_run(fk_batch* b, const fk_item* items, u64 nitems,
+                           int use_graph) {
+  fk_status st = expand(b, items, nitems);
+  if (st) return st;
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    if ((st = upload_items(b))) return st;
+    if ((st = launch(b, use_graph))) return st;
+    st = collect(b);
+    if (st != FK_ERR_OVERFLOW) return st;
+  }
+  return st;
+}
+
+// ------------------------------------------------------------------ C ABI --
+extern "C" {
+
+const char* fk_last_error(void) { return g_err.c_str(); }
+const char* fk_version(void) { return "libfk 1.0 sm_100a"; }
+
+fk_status fk_engine_create(const fk_params* params, fk_engine** out) {
+  if (!params || !out) return set_err(FK_ERR_ARG, "null argument");
+  *out = nullptr;
+  fk_engine* e = new fk_engine();
+  e->p = *params;
+  fk_status st = build_engine(e);
+  if (!st) {
+    e->plain = new fk_batch();
+    st = batch_init(e->plain, &e, 1);
+  }
+  if (st) {
+    fk_engine_destroy(e);
+    return st;
+  }
+  *out = e;
+  return FK_OK;
+}
+
+void fk_engine_destroy(fk_engine* e) {
+  if (!e) return;
+  if (e->plain) { batch_free(e->plain); delete e->plain; }
+  for (void* p : e->allocs) cudaFree(p);
+  delete e;
+}
+
+fk_status fk_engine_info(const fk_engine* e, fk_info* out) {
+  if (!e || !out) return set_err(FK_ERR_ARG, "null argument");
+  out->M = e->M;
+  out->W = e->W;
+  out->L = (uint32_t)e->lanes.size();
+  out->NP = (uint32_t)e->sieve.size();
+  out->first_prime = first_sieve_prime(e);
+  out->nrounds = e->dev.nrounds;
+  out->device_bytes = e->device_bytes;
+  return FK_OK;
+}
+
+static fk_status plain_run(fk_engine* e, const uint64_t lo[2],
+                           const uint64_t hi[2], u32 mode, u32 threshold,
+                           u32 cap, fk_result* out) {
+  if (!e || !lo || !hi || !out) return set_err(FK_ERR_ARG, "null argument");
+  fk_item it{};
+  it.engine = 0;
+  it.mode = mode;
+  it.threshold = threshold;
+  it.cap = cap;
+  it.lo[0] = lo[0]; it.lo[1] = lo[1];
+  it.hi[0] = hi[0]; it.hi[1] = hi[1];
+  fk_status st = batch_run(e->plain, &it, 1, 0);
+  if (st) return st;
+  fk_batch* b = e->plain;
+  out->count = b->r_off.size();
+  out->offset = b->r_off.data();
+  out->depth = b->r_depth.data();
+  return FK_OK;
+}
+
+fk_status fk_sieve(fk_engine* e, const uint64_t lo[2], const uint64_t hi[2],
+                   fk_result* out) {
+  return plain_run(e, lo, hi, MODE_SIEVE, 0, 0, out);
+}
+
+fk_status fk_hunt(fk_engine* e, const uint64_t lo[2], const uint64_t hi[2],
+                  uint32_t threshold, uint32_t cap, fk_result* out) {
+  return plain_run(e, lo, hi, MODE_HUNT, threshold, cap, out);
+}
+
+fk_status fk_dense(fk_engine* e, const uint64_t lo[2], const uint64_t hi[2],
+                   uint32_t threshold, uint32_t cap, fk_result* out) {
+  return plain_run(e, lo, hi, MODE_DENSE, threshold, cap, out);
+}
+
+fk_status fk_batch_create(fk_engine* const* engines, uint32_t nengines,
+                          fk_batch** out) {
+  if (!engines || !out || nengines == 0) return set_err(FK_ERR_ARG, "null argument");
+  *out = nullptr;
+  fk_batch* b = new fk_batch();
+  fk_status st = batch_init(b, engines, nengines);
+  if (st) { batch_free(b); delete b; return st; }
+  *out = b;
+  return FK_OK;
+}
+
+void fk_batch_destroy(fk_batch* b) {
+  if (!b) return;
+  batch_free(b);
+  delete b;
+}
+
+static void fill_result(fk_batch* b, fk_batch_result* out) {
+  out->nitems = b->user.size();
+  out->item_start = b->r_start.data();
+  out->offset = b->r_off.data();
+  out->depth = b->r_depth.data();
+}
+
+fk_status fk_batch_run(fk_batch* b, const fk_item* items, uint64_t nitems,
+                       int use_graph, fk_batch_result* out) {
+  if (!b || (!items && nitems) || !out) return set_err(FK_ERR_ARG, "null argument");
+  fk_status st = batch_run(b, items, nitems, use_graph);
+  if (st) return st;
+  fill_result(b, out);
+  return FK_OK;
+}
+
+fk_status fk_batch_submit(fk_batch* b, const fk_item* items, uint64_t nitems,
+                          int use_graph) {
+  if (!b || (!items && nitems)) return set_err(FK_ERR_ARG, "null argument");
+  if (b->pending) return set_err(FK_ERR_ARG, "a run is already pending");
+  fk_status st = expand(b, items, nitems);
+  if (st) return st;
+  if ((st = upload_items(b))) return st;
+  if ((st = launch(b, use_graph))) return st;
+  b->pending = true;
+  b->pending_graph = use_graph;
+  return FK_OK;
+}
+
+fk_status fk_batch_wait(fk_batch* b, fk_batch_result* out) {
+  if (!b || !out) return set_err(FK_ERR_ARG, "null argument");
+  if (!b->pending) return set_err(FK_ERR_ARG, "nothing pending");
+  b->pending = false;
+  fk_status st = collect(b);
+  for (int attempt = 0; attempt < 3 && st == FK_ERR_OVERFLOW; ++attempt) {
+    if ((st = upload_items(b))) return st;
+    if ((st = launch(b, b->pending_graph))) return st;
+    st = collect(b);
+  }
+  if (st) return st;
+  fill_result(b, out);
+  return FK_OK;
+}
+
+fk_status fk_batch_last_ms(const fk_batch* b, float* sieve_ms,
+                           float* classify_ms, float* total_ms) {
+  if (!b) return set_err(FK_ERR_ARG, "null argument");
+  float a = 0, c = 0, t = 0;
+  FK_CUDA(cudaEventElapsedTime(&a, b->ev[0], b->ev[1]));
+  FK_CUDA(cudaEventElapsedTime(&c, b->ev[1], b->ev[2]));
+  FK_CUDA(cudaEventElapsedTime(&t, b->ev[0], b->ev[3]));
+  if (sieve_ms) *sieve_ms = a;
+  if (classify_ms) *classify_ms = c;
+  if (total_ms) *total_ms = t;
+  return FK_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------- explicit values ---
+__global__ void k_sprp_vals(const u64* v, u64 n, int base2, uint8_t* out) {
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (u64)gridDim.x * blockDim.x) {
+    V3 x = {{v[3 * i], v[3 * i + 1], v[3 * i + 2]}};
+    out[i] = sprp(x, base2 != 0) ? 1 : 0;
+  }
+}
+
+__global__ void k_depth_vals(DevEngine e, const u64* x, u64 n, u32 cap,
+                             uint8_t* out) {
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (u64)gridDim.x * blockDim.x) {
+    const u128 v = ((u128)x[2 * i + 1] << 64) | x[2 * i];
+    u32 depth = 0;
+    if (e.kind == KIND_EULER) {
+      depth = euler_first_fail(v, cap);
+    } else if (e.kind == KIND_DICKSON) {
+      bool of = false;
+      const V3 kk = v3_mul_128(v, v, &of);
+      if (e.two_pass) {
+        depth = dickson_run(kk, cap, true);
+        if (depth >= 5) depth = dickson_run(kk, cap, false);
+      } else {
+        depth = dickson_run(kk, cap, false);
+      }
+      if (of) depth = 255;
+    } else {
+      const V3 d = {{e.d_lo, e.d_hi, 0}};
+      depth = ap_run(v, d, cap, true);
+      if (depth >= 6) depth = ap_run(v, d, cap, false);
+    }
+    out[i] = (uint8_t)min(depth, 255u);
+  }
+}
+
+extern "C" {
+
+fk_status fk_sprp(const uint64_t* v_limbs, uint64_t count, int base2_only,
+                  uint8_t* out) {
+  if ((!v_limbs || !out) && count) return set_err(FK_ERR_ARG, "null argument");
+  if (!count) return FK_OK;
+  u64* dv = nullptr;
+  uint8_t* dout = nullptr;
+  FK_CUDA(cudaMalloc(&dv, count * 24));
+  FK_CUDA(cudaMalloc(&dout, count));
+  FK_CUDA(cudaMemcpy(dv, v_limbs, count * 24, cudaMemcpyHostToDevice));
+  k_sprp_vals<<<(u32)std::min<u64>((count + 255) / 256, 4096), 256>>>(dv, count, base2_only, dout);
+  cudaError_t ce = cudaGetLastError();
+  if (ce == cudaSuccess) ce = cudaMemcpy(out, dout, count, cudaMemcpyDeviceToHost);
+  cudaFree(dv);
+  cudaFree(dout);
+  if (ce != cudaSuccess) return set_err(FK_ERR_DEVICE, cudaGetErrorString(ce));
+  return FK_OK;
+}
+
+fk_status fk_depths(fk_engine* e, const uint64_t* x_limbs, uint64_t count,
+                    uint32_t cap, uint8_t* depth_out) {
+  if (!e || ((!x_limbs || !depth_out) && count)) return set_err(FK_ERR_ARG, "null argument");
+  if (!count) return FK_OK;
+  if (cap > 250) return set_err(FK_ERR_DOMAIN, "cap above 250");
+  for (u64 i = 0; i < count; ++i)
+    if (!chain_fits(e, u128_of(x_limbs + 2 * i), cap, true))
+      return set_err(FK_ERR_DOMAIN, "values past 190 bits");
+  u64* dx = nullptr;
+  uint8_t* dout = nullptr;
+  FK_CUDA(cudaMalloc(&dx, count * 16));
+  FK_CUDA(cudaMalloc(&dout, count));
+  FK_CUDA(cudaMemcpy(dx, x_limbs, count * 16, cudaMemcpyHostToDevice));
+  k_depth_vals<<<(u32)std::min<u64>((count + 255) / 256, 4096), 256>>>(e->dev, dx, count, cap, dout);
+  cudaError_t ce = cudaGetLastError();
+  if (ce == cudaSuccess) ce = cudaMemcpy(depth_out, dout, count, cudaMemcpyDeviceToHost);
+  cudaFree(dx);
+  cudaFree(dout);
+  if (ce != cudaSuccess) return set_err(FK_ERR_DEVICE, cudaGetErrorString(ce));
+  return FK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,382 @@
+// fk_sieve.cuh -- the fused sieve kernel (stages S1 and S2).
+//
+// The line of one item is x = X0 + u*M + R[l]: period u in [0, U), lane l
+// over the wheel's admissible residues R mod M.  A CHAIN is one lane over
+// Tc consecutive 64-period words; one thread runs one chain, a CTA runs
+// 256 chains (a TASK), and a persistent grid pulls tasks from a device
+// counter, so thousands of items of uneven length run in one launch.
+//
+// S1 (pattern sieve).  For the NS pattern primes starting at prime index
+// P0 -- compile-time constants, so each prime's modulus, word step and
+// table offset are immediates -- the kill pattern of 64 consecutive
+// periods of a lane is one 64-bit word of a per-prime table of q words,
+// indexed by the lane's rotating phase rho (u + s_l) mod q.  The tables
+// sit in shared memory, staged from HBM by a bulk async copy (TMA).  This
+// is the reference's stage-1a bit-sieve (euler-prime-runs/euler_gpu.py:
+// 438-520, dickson-ladders/ladder_gpu.py:254-317, and the AP register
+// gather primorial-ap/ap_gpu.py:204-313), re-indexed so that one table per
+// prime serves every lane of every wheel.
+//
+// S2 (compaction rounds).  S1 survivors go to a per-CTA shared-memory
+// queue (block-wide ballot/prefix compaction).  When it fills, the CTA
+// drains it through rounds over the remaining primes: every live candidate
+// is tested against a round's primes (Barrett residue plus the engine's
+// kill test), then survivors are compacted so the next round starts with
+// every lane busy -- the reference's stage 1b / stage 2 rounds
+// (euler-prime-runs/euler_gpu.py:523-709, dickson-ladders/ladder_gpu.py:
+// 349-407) without a host-visible queue.  Final survivors are appended to
+// a global candidate list with warp-aggregated atomics.
+#pragma once
+#include "fk_arith.cuh"
+#include "fk_types.h"
+
+namespace fk {
+
+constexpr u32 kWaitSpins = 1u << 20;
+
+__device__ __forceinline__ u32 smem_u32(const void* p) {
+  return (u32)__cvta_generic_to_shared(p);
+}
+
+// Block-wide exclusive scan of one u32 per thread; returns the prefix and
+// sets *total.  Two barriers.
+__device__ __forceinline__ u32 block_scan(u32 v, u32* s_warp, u32* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  u32 x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    u32 y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[wid] = x;
+  __syncthreads();
+  u32 base = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < kBlock / 32; ++w) {
+    u32 t = s_warp[w];
+    base += (w < wid) ? t : 0;
+    tot += t;
+  }
+  __syncthreads();
+  *total = tot;
+  return base + x - v;
+}
+
+// ---- per-candidate kill tests ------------------------------------------
+// aux bit 31 set: explicit list, offset in bits 0..23, count in 24..30.
+__device__ __forceinline__ bool list_kill(u32 aux, u32 r,
+                                          const u32* __restrict__ lists) {
+  const u32 off = aux & 0x00FFFFFFu, cnt = (aux >> 24) & 0x7Fu;
+  bool k = false;
+  for (u32 c = 0; c < cnt; ++c) k |= (__ldg(lists + off + c) == r);
+  return k;
+}
+
+template <int KIND>
+__device__ __forceinline__ bool kill_test(const PrimeRec& pr, u32 r,
+                                          const u32* __restrict__ lists,
+                                          const u32* s_sbits, u32 xxmax,
+                                          u32 n) {
+  if (pr.aux & 0x80000000u) return list_kill(pr.aux, r, lists);
+  if (KIND == KIND_EULER) {
+    // q > max(x^2+x): r is killed iff q - r (mod q) is one of the x^2+x.
+    if (r == 0) return true;
+    const u32 t = pr.q - r;
+    return t <= xxmax && ((s_sbits[t >> 5] >> (t & 31)) & 1u);
+  } else if (KIND == KIND_AP) {
+    // killed iff r + j*d == 0 (mod q) for some j < n, i.e.
+    // j = (q - r) * d^-1 mod q is below n; aux = d^-1 (0 when q | d).
+    if (r == 0) return true;
+    if (pr.aux == 0) return false;
+    const u32 t = fk_mulmod(pr.q - r, pr.aux, pr.q, pr.magic);
+    return t < n;
+  }
+  return false;  // Dickson primes always carry a list
+}
+
+// ---- S1 helpers, unrolled over the compile-time pattern primes ----------
+template <int P0, int I, int NS>
+struct Pat {
+  static __device__ __forceinline__ void word(const u64* __restrict__ spat,
+                                              u32* rho, u64& acc) {
+    constexpr u32 q = fk_nth_prime(P0 + I);
+    constexpr u32 off = fk_pat_prefix(P0, I);
+    constexpr u32 st = 64u % q;
+    acc |= spat[off + rho[I]];
+    const u32 a = rho[I] + st;
+    rho[I] = min(a, a - q);  // unsigned: a - q wraps when a < q
+    Pat<P0, I + 1, NS>::word(spat, rho, acc);
+  }
+  static __device__ __forceinline__ void setup(u32* rho, u64 R, u64 u0,
+                                               const u32* __restrict__ xq,
+                                               const u32* s_minv) {
+    constexpr u32 q = fk_nth_prime(P0 + I);
+    const u32 rq = (u32)(R % q);
+    const u32 s = (u32)(((xq[I] + rq) % q) * (u64)s_minv[I] % q);
+    rho[I] = (u32)((u0 % q + s) % q);
+    Pat<P0, I + 1, NS>::setup(rho, R, u0, xq, s_minv);
+  }
+};
+template <int P0, int NS>
+struct Pat<P0, NS, NS> {
+  static __device__ __forceinline__ void word(const u64*, u32*, u64&) {}
+  static __device__ __forceinline__ void setup(u32*, u64, u64, const u32*,
+                                               const u32*) {}
+};
+
+struct SieveArgs {
+  const DevEngine* engines;
+  const DevItem* items;
+  const u64* task_prefix;  // [nitems + 1] for this kernel's items
+  const u32* item_index;   // [nitems] global item index of each entry
+  u32 nitems;
+  u32 pad;
+  u64 ntask;
+  const u32* xq;
+  u64* cand_key;
+  u32* cand_item;
+  u64 cand_cap;
+  DevCounters* ctr;
+  unsigned long long* task_ctr;
+};
+
+struct SieveSmem {
+  u32 qa[kQcap];
+  u32 qb[kQcap];
+  u64 chain_R[kBlock];
+  u64 chain_w0[kBlock];
+  u32 warp[kBlock / 32];
+  u32 minv[kNS];
+  u32 sbits[512];
+  u64 task;
+  u32 item;
+  u32 eng;
+  u32 status;
+  u32 pad;
+  unsigned long long mbar;
+};
+
+template <int P0>
+__host__ __device__ constexpr u32 pat_bytes() {
+  return ((fk_pat_prefix(P0, kNS) + 1) / 2) * 16;  // padded to 16 bytes
+}
+
+// Drain the queue: rounds over the per-candidate primes, then append the
+// survivors to the global candidate list.
+template <int KIND>
+__device__ void drain(SieveSmem& S, u32 n, const DevEngine& e,
+                      const DevItem& it, u32 gitem, const SieveArgs& a) {
+  u32* qin = S.qa;
+  u32* qout = S.qb;
+  const u32* __restrict__ xq = a.xq + it.xq_off;
+  const u64 M = e.M;
+  for (u32 r = 0; r < e.nrounds && n > 0; ++r) {
+    const u32 i0 = __ldg(e.rounds + r), i1 = __ldg(e.rounds + r + 1);
+    u32 mask = 0;
+    int k = 0;
+    for (u32 idx = threadIdx.x; idx < n; idx += kBlock, ++k) {
+      const u32 code = qin[idx];
+      const u32 t = code >> 22;
+      const u64 u = 64ull * (S.chain_w0[t] + ((code >> 6) & 0xFFFFu)) +
+                    (code & 63u);
+      const u64 v = u * M + S.chain_R[t];
+      bool alive = true;
+      for (u32 i = i0; i < i1; ++i) {
+        const PrimeRec pr = e.recs[i];
+        u32 rr = fk_bmod(v, pr.q, pr.magic) + __ldg(xq + i);
+        rr = min(rr, rr - pr.q);
+        if (kill_test<KIND>(pr, rr, e.lists, S.sbits, e.xxmax, e.n)) {
+          alive = false;
+          break;
+        }
+      }
+      mask |= (u32)alive << k;
+    }
+    u32 tot;
+    u32 pos = block_scan(__popc(mask), S.warp, &tot);
+    k = 0;
+    for (u32 idx = threadIdx.x; idx < n; idx += kBlock, ++k)
+      if ((mask >> k) & 1u) qout[pos++] = qin[idx];
+    __syncthreads();
+    u32* t = qin;
+    qin = qout;
+    qout = t;
+    n = tot;
+  }
+  // emit survivors
+  for (u32 idx = threadIdx.x; idx < n; idx += kBlock) {
+    const u32 code = qin[idx];
+    const u32 t = code >> 22;
+    const u64 u = 64ull * (S.chain_w0[t] + ((code >> 6) & 0xFFFFu)) +
+                  (code & 63u);
+    const u64 v = u * M + S.chain_R[t];
+    const u32 act = __activemask();
+    const int leader = __ffs(act) - 1;
+    const u32 lanemask = (1u << (threadIdx.x & 31)) - 1;
+    unsigned long long base = 0;
+    if ((int)(threadIdx.x & 31) == leader)
+      base = atomicAdd(&a.ctr->ncand, (unsigned long long)__popc(act));
+    base = __shfl_sync(act, base, leader);
+    const u64 p = base + __popc(act & lanemask);
+    if (p < a.cand_cap) {
+      a.cand_key[p] = v;
+      a.cand_item[p] = gitem;
+    } else {
+      atomicOr(&a.ctr->overflow, 1u);
+    }
+  }
+  __syncthreads();
+}
+
+template <int P0>
+__global__ void __launch_bounds__(kBlock, 2) k_sieve(SieveArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  u64* spat = reinterpret_cast<u64*>(smem_raw);
+  SieveSmem& S = *reinterpret_cast<SieveSmem*>(smem_raw + pat_bytes<P0>());
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    S.eng = 0xFFFFFFFFu;
+    const u32 mb = smem_u32(&S.mbar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb)
+                 : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  u32 phase = 0;
+
+  for (;;) {
+    if (tid == 0) {
+      const u64 t = atomicAdd(a.task_ctr, 1ull);
+      S.task = t;
+      if (t < a.ntask) {
+        // binary search: last entry with task_prefix[i] <= t
+        u32 lo = 0, hi = a.nitems;
+        while (hi - lo > 1) {
+          const u32 mid = (lo + hi) >> 1;
+          if (a.task_prefix[mid] <= t) lo = mid; else hi = mid;
+        }
+        S.item = lo;
+      }
+    }
+    __syncthreads();
+    const u64 task = S.task;
+    if (task >= a.ntask) break;
+    const u32 gitem = a.item_index[S.item];
+    const DevItem it = a.items[gitem];
+    const u32 eidx = it.engine;
+    const DevEngine& eg = a.engines[eidx];
+    // ---- engine switch: stage its pattern table into shared memory ----
+    if (S.eng != eidx) {
+      __syncthreads();
+      if (tid == 0) {
+        S.status = 0;
+        const u32 mb = smem_u32(&S.mbar);
+        const u32 bytes = pat_bytes<P0>();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile(
+            "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb),
+            "r"(bytes)
+            : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
+            " [%0], [%1], %2, [%3];" ::"r"(smem_u32(spat)),
+            "l"((u64)__cvta_generic_to_global(eg.pat)), "r"(bytes), "r"(mb)
+            : "memory");
+        u32 done = 0, spins = 0;
+        while (!done) {
+          asm volatile(
+              "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, "
+              "[%1], %2; selp.u32 %0, 1, 0, p; }"
+              : "=r"(done)
+              : "r"(mb), "r"(phase)
+              : "memory");
+          if (!done && ++spins > kWaitSpins) break;
+        }
+        if (!done) {
+          S.status = 1;
+          atomicOr(&a.ctr->overflow, 4u);
+        }
+      }
+      for (u32 i = tid; i < kNS; i += kBlock) S.minv[i] = eg.pat_minv[i];
+      for (u32 i = tid; i < eg.sbits_words && i < 512; i += kBlock)
+        S.sbits[i] = eg.sbits[i];
+      phase ^= 1u;
+      __syncthreads();
+      if (S.status) return;
+      if (tid == 0) S.eng = eidx;
+    }
+    const DevEngine e = eg;
+    // ---- this thread's chain -------------------------------------------
+    const u64 g = (task - a.task_prefix[S.item]) * kBlock + tid;
+    const u64 nchain = it.nchunk * e.L;
+    const bool active = g < nchain;
+    const u64 chunk = active ? g / e.L : 0;
+    const u32 lane = active ? (u32)(g % e.L) : 0;
+    const u64 R = active ? e.lanes[lane] : 0;
+    const u64 w0 = chunk * it.Tc;
+    S.chain_R[tid] = R;
+    S.chain_w0[tid] = w0;
+    u32 rho[kNS];
+    Pat<P0, 0, kNS>::setup(rho, R, 64ull * w0, a.xq + it.xq_off, S.minv);
+    const u64 U = it.U;
+    u32 qn = 0;
+    __syncthreads();
+    for (u32 wi = 0; wi < it.Tc; ++wi) {
+      const u64 w = w0 + wi;
+      u64 surv = 0;
+      if (active && 64ull * w < U) {
+        u64 acc = 0;
+        Pat<P0, 0, kNS>::word(spat, rho, acc);
+        const u64 left = U - 64ull * w;
+        u64 valid = left >= 64 ? ~0ull : ((1ull << left) - 1ull);
+        if (w == 0 && R < it.lo_off) valid &= ~1ull;
+        if (left <= 64 && R >= it.hi_last) valid &= ~(1ull << (left - 1));
+        surv = ~acc & valid;
+      }
+      // push this word's survivors; drain first when they do not fit, and
+      // when one word-step alone overfills the queue, push the prefix that
+      // fits and drain again (every pass pushes or drains, so it ends)
+      for (;;) {
+        const u32 c = __popcll(surv);
+        u32 tot;
+        u32 pos = block_scan(c, S.warp, &tot);
+        if (tot == 0) break;
+        if (qn + tot <= (u32)kQcap) {
+          pos += qn;
+          while (surv) {
+            const int b = __ffsll((long long)surv) - 1;
+            surv &= surv - 1;
+            S.qa[pos++] = ((u32)tid << 22) | (wi << 6) | (u32)b;
+          }
+          qn += tot;
+          break;
+        }
+        if (qn == 0) {
+          u32 room = pos < (u32)kQcap ? min(c, (u32)kQcap - pos) : 0u;
+          while (room--) {
+            const int b = __ffsll((long long)surv) - 1;
+            surv &= surv - 1;
+            S.qa[pos++] = ((u32)tid << 22) | (wi << 6) | (u32)b;
+          }
+          qn = kQcap;
+        }
+        __syncthreads();
+        switch (e.kind) {
+          case KIND_EULER: drain<KIND_EULER>(S, qn, e, it, gitem, a); break;
+          case KIND_DICKSON: drain<KIND_DICKSON>(S, qn, e, it, gitem, a); break;
+          default: drain<KIND_AP>(S, qn, e, it, gitem, a); break;
+        }
+        qn = 0;
+      }
+      __syncthreads();
+    }
+    switch (e.kind) {
+      case KIND_EULER: drain<KIND_EULER>(S, qn, e, it, gitem, a); break;
+      case KIND_DICKSON: drain<KIND_DICKSON>(S, qn, e, it, gitem, a); break;
+      default: drain<KIND_AP>(S, qn, e, it, gitem, a); break;
+    }
+  }
+}
+
+}  // namespace fk

@@ -1,0 +1,75 @@
+// fk_types.h -- device-side descriptors shared by host and kernels.
+#pragma once
+#include <cstdint>
+
+namespace fk {
+
+enum Kind : uint32_t { KIND_EULER = 0, KIND_DICKSON = 1, KIND_AP = 2 };
+
+// What an item asks for.
+enum Mode : uint32_t {
+  MODE_SIEVE = 0,   // pre-primality survivors only
+  MODE_HUNT = 1,    // survivors classified; keep depth >= threshold
+  MODE_DENSE = 2,   // no sieve: every x in the range is classified
+};
+
+// Per-prime record for the per-candidate stage (16 bytes).
+struct PrimeRec {
+  uint32_t q;
+  uint32_t aux;     // kind test data (see fk_engine.cu, build_tests)
+  uint64_t magic;   // floor(2^64 / q)
+};
+
+constexpr int kBlock = 256;       // threads per CTA, every kernel
+constexpr int kQcap = 4096;       // per-CTA candidate queue (entries)
+constexpr int kNS = 32;           // pattern primes per chain
+constexpr int kMaxRounds = 64;
+constexpr int kSortSmem = 4096;   // entries a CTA sorts in shared memory
+
+// Immutable per-engine tables (device-resident for the engine's life).
+struct DevEngine {
+  uint32_t kind, n, L, NP;        // NP: sieve primes (pattern + per-candidate)
+  uint32_t P0, NS, nrounds, xxmax;
+  uint32_t pat_words, sbits_words, two_pass, pad0;
+  uint64_t M;                     // wheel period (x units)
+  uint64_t W;                     // Dickson: k = W * j
+  uint64_t d_lo, d_hi;            // AP difference
+  const uint64_t* lanes;          // [L] admissible residues mod M, ascending
+  const uint64_t* pat;            // pattern words, compile-time layout
+  const uint32_t* pat_minv;       // [NS] (M mod q)^-1 mod q
+  const PrimeRec* recs;           // [NP]
+  const uint32_t* c64;            // [NP] 2^64 mod q
+  const uint32_t* lists;          // explicit forbidden-residue lists
+  const uint32_t* rounds;         // [nrounds + 1] prime-index cuts
+  const uint32_t* sbits;          // Euler: bitset of {x^2 + x : x < n}
+};
+
+// One unit of work: a sub-range of one engine's line.
+struct DevItem {
+  uint32_t engine, mode, threshold, cap;
+  uint64_t X0_lo, X0_hi;          // line base (a multiple of M for sieves)
+  uint64_t U;                     // periods (sieve) or x count (dense)
+  uint64_t lo_off;                // first valid x - X0 (in period 0)
+  uint64_t hi_last;               // valid iff R < hi_last in period U-1
+  uint32_t Tc, pad1;              // words per chain
+  uint64_t nchunk;                // chains per lane
+  uint64_t task0, ntask;          // first task, task count
+  uint64_t xq_off;                // this item's base-residue table
+};
+
+// Output entry before ordering: item index + (key << 8 | depth).
+struct OutRec {
+  uint64_t packed;
+  uint32_t item;
+  uint32_t pad;
+};
+
+struct DevCounters {
+  unsigned long long task_next;   // persistent task counter
+  unsigned long long ncand;       // candidates written
+  unsigned long long nout;        // outputs written
+  unsigned int overflow;          // bit 0 cand, bit 1 out, bit 2 timeout
+  unsigned int pad;
+};
+
+}  // namespace fk

@@ -1,0 +1,159 @@
+/* fk.h -- C ABI of libfk, the B200 sieve + strong-probable-prime engine for
+ * the three prime-constellation hunts of jhg023/first-knowns:
+ *
+ *   FK_EULER    Euler-form runs      x^2 + x + p          (line variable p)
+ *   FK_DICKSON  Dickson ladders      m*k^2 + 1, k = W*j   (line variable j)
+ *   FK_AP       primorial-step APs   p + i*d              (line variable p)
+ *
+ * The reference engines are Python classes (no FFI of their own); each
+ * entry point below replaces one device-side step of them and is what the
+ * ctypes layer in first-knowns_b200/fk_abi.py binds.  Plain pointers and
+ * sizes only.  Line values are unsigned 128-bit integers passed as two
+ * little-endian uint64 limbs.  Results are owned by the engine (or batch)
+ * and stay valid until its next call.  Every call is single-threaded per
+ * handle, as the reference engines are (one host thread per engine).
+ */
+#ifndef FK_H
+#define FK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t fk_status;
+#define FK_OK 0
+#define FK_ERR_DOMAIN 1   /* ValueError in the reference: bad range/params */
+#define FK_ERR_OVERFLOW 2 /* RuntimeError: a queue or buffer overflowed   */
+#define FK_ERR_DEVICE 3   /* CUDA error                                    */
+#define FK_ERR_TIMEOUT 4  /* a bounded device wait gave up                 */
+#define FK_ERR_ARG 5      /* null pointer / invalid handle                 */
+
+#define FK_EULER 0
+#define FK_DICKSON 1
+#define FK_AP 2
+
+typedef struct fk_engine fk_engine;
+typedef struct fk_batch fk_batch;
+
+/* Engine construction parameters.
+ *   Euler:   GpuEngine(n, wheel_primes)  euler-prime-runs/euler_gpu.py:1010
+ *   Dickson: GpuEngine(n, q2, ...)       dickson-ladders/ladder_gpu.py:424
+ *   AP:      GpuEngine(n, q2, launch_u)  primorial-ap/ap_gpu.py:401      */
+typedef struct fk_params {
+  uint32_t kind;      /* FK_EULER / FK_DICKSON / FK_AP                       */
+  uint32_t n;         /* filter: values x^2+x+p for x < n; m = 1..n; AP n     */
+  uint32_t q2;        /* sieve depth: primes below q2 (0: 65536)              */
+  uint32_t p0;        /* first pattern-sieve prime index: 3, 6, 9 or 12       *
+                       * (all sieve primes below it are folded into the       *
+                       * wheel); 0 picks a default for the kind               */
+  uint64_t d_lo, d_hi;/* AP difference (0, 0: the n-th primorial)             */
+  uint32_t two_pass;  /* Dickson: launcher's two-pass sprp_run depth          */
+  uint32_t reserved;
+} fk_params;
+
+/* Read-only description of an engine, for the Python mirrors. */
+typedef struct fk_info {
+  uint64_t M;          /* wheel period of the device line                     */
+  uint64_t W;          /* Dickson k = W*j                                     */
+  uint32_t L;          /* wheel lanes                                         */
+  uint32_t NP;         /* sieve primes                                        */
+  uint32_t first_prime;/* smallest sieve prime not folded into the wheel      */
+  uint32_t nrounds;    /* compaction rounds                                   */
+  uint64_t device_bytes; /* bytes this engine holds on the device             */
+} fk_info;
+
+/* One ordered result: x = base + offset[i]; depth[i] is the chain depth
+ * (0 for pre-primality streams). */
+typedef struct fk_result {
+  uint64_t count;
+  const uint64_t* offset;
+  const uint8_t* depth;
+} fk_result;
+
+/* One interval of a batch. */
+typedef struct fk_item {
+  uint32_t engine;     /* index into the batch's engine list                  */
+  uint32_t mode;       /* 0 sieve stream, 1 hunt (classified), 2 dense        */
+  uint32_t threshold;  /* keep depth >= threshold (hunt / dense)              */
+  uint32_t cap;        /* chain cap                                           */
+  uint64_t lo[2];      /* [lo, hi) in the engine's line variable              */
+  uint64_t hi[2];
+} fk_item;
+
+/* Batch result: per item, its slice of the concatenated ordered stream. */
+typedef struct fk_batch_result {
+  uint64_t nitems;
+  const uint64_t* item_start;  /* [nitems + 1] slice boundaries               */
+  const uint64_t* offset;      /* x - item.lo                                 */
+  const uint8_t* depth;
+} fk_batch_result;
+
+/* ---- engines ---------------------------------------------------------- */
+/* Builds the wheel, pattern tables, per-prime kill tests and compaction
+ * rounds, and uploads them; they stay device-resident until destroy.    */
+fk_status fk_engine_create(const fk_params* params, fk_engine** out);
+void fk_engine_destroy(fk_engine* e);
+fk_status fk_engine_info(const fk_engine* e, fk_info* out);
+
+/* Pre-primality survivor stream of [lo, hi), ascending.
+ * Replaces survivors_pre_mr   euler-prime-runs/euler_gpu.py:1335-1456,
+ *          survivors_j        dickson-ladders/ladder_gpu.py:757-781,
+ *          survivors          primorial-ap/ap_gpu.py:555-635.           */
+fk_status fk_sieve(fk_engine* e, const uint64_t lo[2], const uint64_t hi[2],
+                   fk_result* out);
+
+/* Survivors of [lo, hi) classified on the device; those whose depth
+ * reaches `threshold`, ascending, with depths.
+ * Replaces hunt               euler-prime-runs/euler_gpu.py:1458-1464,
+ *                             dickson-ladders/ladder_gpu.py:819-829,
+ *                             primorial-ap/ap_gpu.py:661-670,
+ * and the host classification pools that follow them in the launchers
+ * (euler-prime-runs/launch.py:664-667, dickson-ladders/launch.py:310-402,
+ * primorial-ap/launch.py:195-234).                                      */
+fk_status fk_hunt(fk_engine* e, const uint64_t lo[2], const uint64_t hi[2],
+                  uint32_t threshold, uint32_t cap, fk_result* out);
+
+/* Every x in [lo, hi) classified directly, no sieve (the launchers' low
+ * passes below the engine floors: euler-prime-runs/launch.py:410-420,
+ * dickson-ladders/launch.py:653-669, where x is k itself).              */
+fk_status fk_dense(fk_engine* e, const uint64_t lo[2], const uint64_t hi[2],
+                   uint32_t threshold, uint32_t cap, fk_result* out);
+
+/* Chain depth of explicit line values (count values, two limbs each).
+ * Replaces chain_depth  primorial-ap/ap_gpu.py:651-659 and run_length
+ * dickson-ladders/ladder_gpu.py:813-817 for caller-supplied values.     */
+fk_status fk_depths(fk_engine* e, const uint64_t* x_limbs, uint64_t count,
+                    uint32_t cap, uint8_t* depth_out);
+
+/* ---- batches: many intervals, one persistent launch per run ---------- */
+fk_status fk_batch_create(fk_engine* const* engines, uint32_t nengines,
+                          fk_batch** out);
+void fk_batch_destroy(fk_batch* b);
+/* Runs all items; use_graph != 0 replays a captured CUDA graph. */
+fk_status fk_batch_run(fk_batch* b, const fk_item* items, uint64_t nitems,
+                       int use_graph, fk_batch_result* out);
+/* Asynchronous form for the serving loop: submit, then wait. */
+fk_status fk_batch_submit(fk_batch* b, const fk_item* items, uint64_t nitems,
+                          int use_graph);
+fk_status fk_batch_wait(fk_batch* b, fk_batch_result* out);
+/* Device time (ms) of the last run's kernels, from CUDA events. */
+fk_status fk_batch_last_ms(const fk_batch* b, float* sieve_ms,
+                           float* classify_ms, float* total_ms);
+
+/* ---- misc -------------------------------------------------------------- */
+/* Last error message on this thread. */
+const char* fk_last_error(void);
+/* Device SPRP verdicts for explicit values (three limbs each):
+ * huntlib/primes.py mr_is_prime (base2_only = 0) / sprp_base2 (1).      */
+fk_status fk_sprp(const uint64_t* v_limbs, uint64_t count, int base2_only,
+                  uint8_t* out);
+/* Library version string. */
+const char* fk_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FK_H */
