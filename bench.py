@@ -1,0 +1,421 @@
+#!/usr/bin/env python3
+"""Benchmark: candidates swept per second, persistent batch vs plain engine.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fk|reference]
+
+One STEP is one sweep of the mixed batch workload: 4096 seeded intervals
+(engine uniform over Euler / Dickson / AP, length 2^U(20,36), threshold
+4..12, start 10^U(10,18)), every survivor classified on the device, the
+ordered (x, depth) stream of every interval returned.  Under torchrun each
+rank sweeps its own 4096 intervals (seed + rank): the intervals are
+independent, so the work shards with no data-path collective (weak
+scaling); torch.distributed only carries the barrier and the max-over-
+ranks time.
+
+Reported (one JSON line, rank 0):
+  value      candidates/s of the batched pipeline, device time from CUDA
+             events on the library's stream (interval table already
+             uploaded when the timed region starts)
+  e2e        the same through the public batch API from host intervals to
+             host results, wall time, copies included
+  plain      the plain per-interval engine on the same intervals (one
+             fk_hunt call each), and batch_over_plain; bit_identical says
+             both streams matched exactly
+  roofline   the dominant kernel against its measured bound (integer
+             multiply-add rate for the SPRP stage, shared-memory load rate
+             for the pattern sieve)
+  cpu_baseline  the CPU oracle (a restatement of the reference's numpy
+             engines) on a bounded sample of the workload, all host cores
+  serve      p50/p99 request latency of the continuous-batching server on
+             the served workload (Poisson arrivals)
+  clocks     SM clock and throttle reasons sampled during the timed region
+
+``--impl reference`` times the reference's CPU implementation of the path
+(its numpy engines, restated in oracle/) on bounded samples of the same
+workload and prints the same line with "impl": "reference".
+"""
+
+import argparse
+import concurrent.futures as cf
+import datetime
+import json
+import multiprocessing as mp
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+for _p in (str(ROOT), str(ROOT / "first-knowns_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = ("candidates/s swept bit-exact: persistent batch vs plain engine; "
+          "p50/p99 latency")
+UNIT = "candidates/s"
+WORKLOAD = ("mixed_batch: 4096 intervals, engine uniform over {Euler x^2+x+p,"
+            " Dickson m*k^2+1, AP p+j*P(n)}, length 2^U(20,36), threshold "
+            "U{4..12}, start 10^U(10,18) (AP aligned to 30), seed 20261203 "
+            "(+rank), sieve to 65536, chains classified on the device")
+SAMPLE_CLIP = 1 << 24
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fk", choices=["fk", "reference"])
+    ap.add_argument("--count", type=int, default=4096)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--serve-seconds", type=float, default=8.0)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- ranks ---
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Dist:
+    def __init__(self, world, local):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import torch
+            import torch.distributed as td
+            torch.cuda.set_device(local)
+            td.init_process_group("nccl", timeout=datetime.timedelta(
+                seconds=300))
+            self.td, self.torch = td, torch
+
+    def barrier(self):
+        if self.world > 1:
+            self.td.barrier()
+
+    def max(self, x):
+        if self.world == 1:
+            return float(x)
+        t = self.torch.tensor([float(x)], device="cuda", dtype=self.torch.float64)
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.td.destroy_process_group()
+
+
+# --------------------------------------------------------------- clocks ---
+
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" +
+                 self.FIELDS, "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = max((num(r[2]) for r in rows if num(r[2]) is not None),
+                 default=None)
+        loaded = [s for s in sm if mx and s > 0.5 * mx] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4)
+                          if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------- CPU sample ---
+
+def cpu_sample(intervals, workers, seed=7):
+    """A bounded sample of the workload: a seeded subset of its intervals,
+    each clipped to SAMPLE_CLIP of the search variable (AP to whole
+    periods of 30)."""
+    import random
+    rng = random.Random(seed)
+    idx = list(range(len(intervals)))
+    rng.shuffle(idx)
+    jobs = []
+    for i in idx[:max(8, 2 * workers)]:
+        iv = intervals[i]
+        hi = min(iv.hi, iv.lo + SAMPLE_CLIP)
+        if iv.kind == 2:
+            hi = iv.lo + max(30, (hi - iv.lo) // 30 * 30)
+        jobs.append((iv.kind, iv.n, iv.lo, hi, iv.threshold, iv.cap, iv.q2,
+                     iv.d))
+    return jobs
+
+
+def run_cpu(pool, jobs):
+    from oracle import sweep
+    t0 = time.perf_counter()
+    res = list(pool.map(sweep.run_job, jobs))
+    dt = time.perf_counter() - t0
+    cands = sum(j[3] - j[2] for j in jobs)
+    return cands, dt, res
+
+
+def cpu_pool(workers):
+    return cf.ProcessPoolExecutor(max_workers=workers,
+                                  mp_context=mp.get_context("spawn"))
+
+
+# ------------------------------------------------------------ reference ---
+
+def bench_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    import fk_workloads as W
+    intervals = W.mixed_batch(args.count, W.SEED)
+    workers = os.cpu_count() or 1
+    jobs = cpu_sample(intervals, workers)
+    with cpu_pool(workers) as pool:
+        for _ in range(args.warmup):
+            run_cpu(pool, jobs)
+        times = []
+        cands = 0
+        for _ in range(args.steps):
+            cands, dt, _ = run_cpu(pool, jobs)
+            times.append(dt)
+    ms = 1e3 * statistics.mean(times)
+    value = cands / (ms * 1e-3)
+    sample = (f"{len(jobs)} of the workload's intervals (seeded subset), each "
+              f"clipped to 2^24 of its search variable: {cands:.4g} "
+              f"candidates per step")
+    line = {"impl": "reference", "metric": METRIC, "value": value,
+            "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "intervals": args.count,
+                       "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ fk ---
+
+def bench_fk(args):
+    rank, world, local = dist_env()
+    dist = Dist(world, local)
+    import torch
+    import fk_abi
+    import fk_workloads as W
+    from fk_batch import BatchEngine, PlainEngine
+
+    torch.cuda.set_device(local)
+    fk_abi.set_device(local)
+    intervals = W.mixed_batch(args.count, W.SEED + rank)
+    cands = W.total_length(intervals)
+    eng = BatchEngine(intervals)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    for _ in range(max(args.warmup, 3)):
+        ref_rows = eng.run(intervals, graph=True)
+    torch.cuda.synchronize()
+
+    clocks = Clocks(local)
+    clocks.start()
+    dev_ms, wall_s, stats = [], [], []
+    for k in range(args.steps):
+        flush.fill_(k & 255)               # L2 flushed between steps
+        torch.cuda.synchronize()
+        dist.barrier()
+        t0 = time.perf_counter()
+        rows = eng.run(intervals, graph=True)
+        t1 = time.perf_counter()
+        torch.cuda.synchronize()
+        st = eng.stats()
+        dev_ms.append(st["total_ms"])
+        wall_s.append(t1 - t0)
+        stats.append(st)
+        if rows != ref_rows:
+            raise RuntimeError("batched stream changed between steps")
+    dist.barrier()
+    clk = clocks.stop()
+
+    t_dev = dist.max(sum(dev_ms) * 1e-3)
+    t_wall = dist.max(sum(wall_s))
+    total = cands * args.steps * world
+    value = total / t_dev
+    e2e = total / t_wall
+    st = stats[-1]
+    st_mean = {k: statistics.mean(s[k] for s in stats)
+               for k in ("sieve_ms", "classify_ms", "total_ms")}
+
+    # plain per-interval engine on the same intervals, bit-exact check
+    plain = None
+    bit_identical = None
+    if not args.no_plain:
+        pe = PlainEngine(eng.engset)
+        pe.run(intervals[:64])                 # warm
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        prow = pe.run(intervals)
+        tp = time.perf_counter() - t0
+        bit_identical = prow == ref_rows
+        tp = dist.max(tp)
+        plain = {"value": cands * world / tp, "unit": UNIT,
+                 "ms_per_step": tp * 1e3,
+                 "calls": len(intervals)}
+
+    # rooflines from the device work counters and measured peaks
+    imad_peak = fk_abi.peak("imad")
+    smem_peak = fk_abi.peak("smem")
+    cls_s = st_mean["classify_ms"] * 1e-3
+    sv_s = st_mean["sieve_ms"] * 1e-3
+    imad_rate = st["imad_alg"] / cls_s if cls_s > 0 else 0.0
+    smem_bytes = st["s1_words"] * 32 * 8
+    smem_rate = smem_bytes / sv_s if sv_s > 0 else 0.0
+    roof_cls = {"kernel": "k_classify (device SPRP chains)", "bound": "imad",
+                "achieved": imad_rate / 1e9, "peak": imad_peak / 1e9,
+                "unit": "G int-multiply-adds/s",
+                "frac": imad_rate / imad_peak if imad_peak else None,
+                "algorithmic": "(bits-1)*(4l^2+2l) per strong-test base, "
+                               "l = ceil(bits/32)",
+                "work_per_launch": st["imad_alg"],
+                "traffic": None,
+                "peak_source": "measured on this GPU by fk_peak (32-bit "
+                               "mad.lo/mad.hi chains)"}
+    roof_sv = {"kernel": "k_sieve (pattern sieve + compaction rounds)",
+               "bound": "smem", "achieved": smem_rate / 1e9,
+               "peak": smem_peak / 1e9, "unit": "GB/s",
+               "frac": smem_rate / smem_peak if smem_peak else None,
+               "algorithmic": "8 B pattern word per pattern prime (32) per "
+                              "64 candidates",
+               "work_per_launch": smem_bytes,
+               "s2_prime_tests": st["s2_tests"], "traffic": None,
+               "peak_source": "measured on this GPU by fk_peak (64-bit "
+                              "conflict-free shared loads)"}
+    dominant, secondary = (roof_sv, roof_cls) if sv_s >= cls_s else \
+        (roof_cls, roof_sv)
+
+    # CPU baseline (rank 0, one GPU): oracle on a bounded sample
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        workers = os.cpu_count() or 1
+        jobs = cpu_sample(intervals, workers)
+        with cpu_pool(workers) as pool:
+            run_cpu(pool, jobs[:workers])       # build tables in workers
+            cc, dt, _ = run_cpu(pool, jobs)
+        cpu = {"value": cc / dt, "unit": UNIT, "cores": workers,
+               "kind": "port",
+               "sample": f"{len(jobs)} seeded intervals of the workload, "
+                         f"each clipped to 2^24: {cc:.4g} candidates in "
+                         f"{dt:.1f} s"}
+
+    # served workload: continuous batching, p50/p99 latency
+    serve = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        import numpy as np
+        from fk_serve import ServeLoop
+        reqs = W.served(count=4000, rate_hz=250.0)
+        loop = ServeLoop(eng.engset, slots=2)
+        res, lat, sst = loop.run(reqs, time_limit=args.serve_seconds)
+        done = ~np.isnan(lat)
+        served_c = sum(reqs[i][1].length for i in np.nonzero(done)[0])
+        serve = {"requests": int(done.sum()),
+                 "p50_ms": float(np.percentile(lat[done], 50) * 1e3),
+                 "p99_ms": float(np.percentile(lat[done], 99) * 1e3),
+                 "throughput": served_c / sst["wall_s"], "unit": UNIT,
+                 "arrival_hz": 250.0, "batches": sst["batches"],
+                 "device_busy_frac": sst["device_busy_s"] / sst["wall_s"]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_dev / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded interval draws; no dataset)",
+            "config": {"workload": WORKLOAD, "intervals": args.count,
+                       "candidates_per_rank_step": cands,
+                       "l2": "flushed between steps (256 MiB write)",
+                       "graph": True, "device_items": st["items"]},
+            "roofline": dominant,
+            "roofline_secondary": secondary,
+            "kernel_ms": st_mean,
+            "work": {k: st[k] for k in ("candidates", "outputs", "s1_words",
+                                       "s2_tests", "imad_alg",
+                                       "sprp_values")},
+            "e2e": {"value": e2e, "unit": UNIT,
+                    "h2d_bytes_per_step": int(st["h2d_bytes"]),
+                    "d2h_bytes_per_step": int(st["d2h_bytes"])},
+            "plain": plain,
+            "batch_over_plain": (value / plain["value"]) if plain else None,
+            "e2e_batch_over_plain": (e2e / plain["value"]) if plain else None,
+            "bit_identical": bit_identical,
+            "cpu_baseline": cpu,
+            "serve": serve,
+            "clocks": clk,
+            "gpu_launches": int(st["launches"]) * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    del eng
+    dist.close()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return bench_reference(args)
+    return bench_fk(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

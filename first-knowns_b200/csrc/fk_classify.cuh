@@ -49,11 +49,11 @@ __device__ __forceinline__ void emit_out(const ClassArgs& a, u32 item,
 
 // Euler: f = first x >= 0 with x^2 + x + p failing mr_is_prime, searched
 // up to lim (euler_search.py:258-262, :349-356).
-__device__ u32 euler_first_fail(u128 p, u32 lim) {
+__device__ u32 euler_first_fail(u128 p, u32 lim, u64* imad) {
   u32 t = 0;
   while (t < lim) {
     const V3 v = v3_from_u128(p + (u128)((u64)t * t + t));
-    if (!sprp(v, false)) break;
+    if (!sprp(v, false, imad)) break;
     ++t;
   }
   return t;
@@ -61,24 +61,24 @@ __device__ u32 euler_first_fail(u128 p, u32 lim) {
 
 // Dickson: r = largest count with m*k^2 + 1 passing for m = 1..r, capped
 // (ladder_search.py:143-148); base2 selects the launcher's first pass.
-__device__ u32 dickson_run(const V3& kk, u32 cap, bool base2) {
+__device__ u32 dickson_run(const V3& kk, u32 cap, bool base2, u64* imad) {
   u32 r = 0;
   while (r < cap) {
     V3 v = v3_mul_u64(kk, (u64)(r + 1));
     V3 one = {{1, 0, 0}};
     v = v3_add(v, one);
-    if (!sprp(v, base2)) break;
+    if (!sprp(v, base2, imad)) break;
     ++r;
   }
   return r;
 }
 
 // AP chain p + j*d from j = 0, capped (ap_search.py:160-194 when two-pass).
-__device__ u32 ap_run(u128 p, const V3& d, u32 cap, bool base2) {
+__device__ u32 ap_run(u128 p, const V3& d, u32 cap, bool base2, u64* imad) {
   u32 j = 0;
   V3 v = v3_from_u128(p);
   while (j < cap) {
-    if (!sprp(v, base2)) break;
+    if (!sprp(v, base2, imad)) break;
     v = v3_add(v, d);
     ++j;
   }
@@ -89,6 +89,7 @@ __global__ void __launch_bounds__(kBlock) k_classify(ClassArgs a) {
   u64 n = a.ctr->ncand;
   if (n > a.cand_cap) n = a.cand_cap;
   const u64 stride = (u64)gridDim.x * blockDim.x;
+  u64 imad = 0, nval = 0;
   for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += stride) {
     const u32 item = a.cand_item[i];
@@ -104,7 +105,8 @@ __global__ void __launch_bounds__(kBlock) k_classify(ClassArgs a) {
     bool keep = false;
     if (e.kind == KIND_EULER) {
       const u32 lim = max(it.threshold, it.cap);
-      const u32 f = euler_first_fail(x, lim);
+      const u32 f = euler_first_fail(x, lim, &imad);
+      nval += min(f + 1, lim);
       depth = min(f, it.cap);
       keep = (it.mode == MODE_DENSE) ? depth >= it.threshold
                                      : f >= it.threshold;
@@ -119,19 +121,39 @@ __global__ void __launch_bounds__(kBlock) k_classify(ClassArgs a) {
         continue;
       }
       if (e.two_pass) {
-        depth = dickson_run(kk, it.cap, true);
-        if (depth >= 5) depth = dickson_run(kk, it.cap, false);
+        depth = dickson_run(kk, it.cap, true, &imad);
+        nval += min(depth + 1, it.cap);
+        if (depth >= 5) {
+          depth = dickson_run(kk, it.cap, false, &imad);
+          nval += min(depth + 1, it.cap);
+        }
       } else {
-        depth = dickson_run(kk, it.cap, false);
+        depth = dickson_run(kk, it.cap, false, &imad);
+        nval += min(depth + 1, it.cap);
       }
       keep = depth >= it.threshold;
     } else {
       const V3 d = {{e.d_lo, e.d_hi, 0}};
-      depth = ap_run(x, d, it.cap, true);
-      if (depth >= 6) depth = ap_run(x, d, it.cap, false);
+      depth = ap_run(x, d, it.cap, true, &imad);
+      nval += min(depth + 1, it.cap);
+      if (depth >= 6) {
+        depth = ap_run(x, d, it.cap, false, &imad);
+        nval += min(depth + 1, it.cap);
+      }
       keep = depth >= it.threshold;
     }
     if (keep) emit_out(a, item, (v << 8) | (u64)min(depth, 255u));
+  }
+  // one atomic per warp for the work counters
+  u64 s1 = imad, s2 = nval;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s1 += __shfl_down_sync(0xffffffffu, s1, o);
+    s2 += __shfl_down_sync(0xffffffffu, s2, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (s1) atomicAdd(&a.ctr->imad_alg, (unsigned long long)s1);
+    if (s2) atomicAdd(&a.ctr->sprp_values, (unsigned long long)s2);
   }
 }
 

@@ -16,6 +16,7 @@
 #include "../../include/fk.h"
 #include "fk_arith.cuh"
 #include "fk_classify.cuh"
+#include "fk_mark.cuh"
 #include "fk_sieve.cuh"
 #include "fk_types.h"
 
@@ -119,6 +120,9 @@ struct fk_engine {
   std::vector<u32> sieve;     // pattern primes, then per-candidate primes
   std::vector<std::vector<u32>> forb;  // forbidden residues of x mod q
   double survival = 1.0;      // expected survival through every sieve prime
+  bool use_mark = false;      // long lanes go to the marking sieve
+  bool force_mark = false;    // every item goes to the marking sieve
+  double test_cost = 0, mark_cost = 0;
   DevEngine dev{};
   std::vector<void*> allocs;
   u64 device_bytes = 0;
@@ -126,6 +130,14 @@ struct fk_engine {
   std::vector<uint64_t> res_off;
   std::vector<uint8_t> res_depth;
 };
+
+// End of the marked prime range: primes below 2^16 (their lane shifts are
+// stored as u16), at most 8192 of them past the pattern primes.
+static u32 NS_marked_end(const fk_engine* e) {
+  u32 i = kNS;
+  while (i < e->sieve.size() && e->sieve[i] < 65536u && i - kNS < 8192u) ++i;
+  return i;
+}
 
 static u32 first_sieve_prime(const fk_engine* e) {
   return e->sieve.empty() ? 0 : e->sieve[0];
@@ -343,6 +355,44 @@ static fk_status build_engine(fk_engine* e) {
     rounds.push_back(NP);
   }
   if (NP <= (u32)kNS) rounds.assign({(u32)kNS, (u32)kNS});
+  // ---- marking tables: u-residue lists for every prime, (M mod q)^-1 ------
+  std::vector<u32> minv_all(NP), gaux(NP), glist;
+  u32 NPm = NS_marked_end(e);
+  for (u32 i = 0; i < NP; ++i) {
+    const u32 q = e->sieve[i];
+    const u64 mi = invmod(e->M % q, q);
+    minv_all[i] = (u32)mi;
+    const auto& f = e->forb[i];
+    if (f.size() > 127) return set_err(FK_ERR_DOMAIN, "forbidden set too large");
+    gaux[i] = (u32)glist.size() | ((u32)f.size() << 24);
+    std::vector<u32> g;
+    for (u32 r : f) g.push_back((u32)mulmod64(r, mi, q));
+    std::sort(g.begin(), g.end());
+    glist.insert(glist.end(), g.begin(), g.end());
+  }
+  if (glist.size() >= (1u << 24)) return set_err(FK_ERR_DOMAIN, "glist too large");
+  // cost model (instructions per post-wheel candidate): per-candidate
+  // rounds test every survivor against every remaining prime; marking
+  // pays one byte store per hit plus a per-segment setup per prime
+  {
+    double test_cost = 0, mark_cost = 0, surv = 1.0;
+    for (u32 i = kNS; i < NP; ++i) {
+      const double kill = (double)e->forb[i].size() / e->sieve[i];
+      test_cost += 22.0 * surv;
+      if (i < NPm) {
+        mark_cost += 4.0 * kill + (12.0 + 4.0 * e->forb[i].size()) / kSeg;
+      } else {
+        mark_cost += 22.0 * surv;
+      }
+      surv *= 1.0 - kill;
+    }
+    e->use_mark = NPm > (u32)kNS && mark_cost < test_cost;
+    if (p.sieve == 1) e->use_mark = false;
+    if (p.sieve == 2) e->use_mark = NPm > (u32)kNS;
+    e->force_mark = p.sieve == 2 && e->use_mark;
+    e->test_cost = test_cost;
+    e->mark_cost = mark_cost;
+  }
   // ---- upload -------------------------------------------------------------
   DevEngine& d = e->dev;
   d.kind = e->kind;
@@ -369,6 +419,11 @@ static fk_status build_engine(fk_engine* e) {
   if ((st = upload(e, lists, &d.lists))) return st;
   if ((st = upload(e, rounds, &d.rounds))) return st;
   if ((st = upload(e, sbits, &d.sbits))) return st;
+  d.NPm = NPm;
+  d.use_mark = e->use_mark ? 1 : 0;
+  if ((st = upload(e, minv_all, &d.minv_all))) return st;
+  if ((st = upload(e, gaux, &d.gaux))) return st;
+  if ((st = upload(e, glist, &d.glist))) return st;
   return FK_OK;
 }
 
@@ -422,6 +477,7 @@ struct SubItem {
 
 struct Family {
   u32 P0;
+  bool mark = false;
   std::vector<u32> idx;         // internal item indices
   std::vector<u64> prefix;      // task prefix, size idx+1
   DevBuf<u32> d_idx;
@@ -438,7 +494,7 @@ struct fk_batch {
   std::vector<DevItem> items;
   std::vector<SubItem> sub;
   std::vector<u32> dense_idx, sieve_idx;
-  Family fam[4];
+  Family fam[8];
   // device buffers
   DevBuf<DevItem> d_items;
   DevBuf<u32> d_dense, d_sieve;
@@ -467,6 +523,8 @@ struct fk_batch {
   std::vector<uint8_t> r_depth;
   bool pending = false;
   int pending_graph = 0;
+  u64 last_launches = 0;
+  u64 h2d = 0, d2h = 0;
 };
 
 static const int kOccupancy = 2;
@@ -486,8 +544,11 @@ static fk_status batch_init(fk_batch* b, fk_engine* const* engines,
   FK_CUDA(cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, dev));
   for (int i = 0; i < 4; ++i) FK_CUDA(cudaEventCreate(&b->ev[i]));
   const u32 P0s[4] = {3, 6, 9, 12};
-  for (int f = 0; f < 4; ++f) b->fam[f].P0 = P0s[f];
-  FK_CUDA(b->d_task_ctr.ensure(4) == FK_OK ? cudaSuccess : cudaErrorMemoryAllocation);
+  for (int f = 0; f < 8; ++f) {
+    b->fam[f].P0 = P0s[f & 3];
+    b->fam[f].mark = f >= 4;
+  }
+  FK_CUDA(b->d_task_ctr.ensure(8) == FK_OK ? cudaSuccess : cudaErrorMemoryAllocation);
   FK_CUDA(b->d_nitems.ensure(4) == FK_OK ? cudaSuccess : cudaErrorMemoryAllocation);
   FK_CUDA(b->h_ctr.ensure(1) == FK_OK ? cudaSuccess : cudaErrorMemoryAllocation);
   static bool attrs_done = false;
@@ -500,6 +561,14 @@ static fk_status batch_init(fk_batch* b, fk_engine* const* engines,
                                  (int)(pat_bytes<9>() + sizeof(SieveSmem))));
     FK_CUDA(cudaFuncSetAttribute(k_sieve<12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(pat_bytes<12>() + sizeof(SieveSmem))));
+    FK_CUDA(cudaFuncSetAttribute(k_mark<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(pat_bytes<3>() + sizeof(MarkSmem))));
+    FK_CUDA(cudaFuncSetAttribute(k_mark<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(pat_bytes<6>() + sizeof(MarkSmem))));
+    FK_CUDA(cudaFuncSetAttribute(k_mark<9>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(pat_bytes<9>() + sizeof(MarkSmem))));
+    FK_CUDA(cudaFuncSetAttribute(k_mark<12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(pat_bytes<12>() + sizeof(MarkSmem))));
     attrs_done = true;
   }
   return FK_OK;
@@ -522,7 +591,12 @@ static void batch_free(fk_batch* b) {
   if (b->stream) cudaStreamDestroy(b->stream);
 }
 
-static int fam_of(u32 P0) { return P0 == 3 ? 0 : P0 == 6 ? 1 : P0 == 9 ? 2 : 3; }
+static int fam_of(u32 P0, bool mark) {
+  return (P0 == 3 ? 0 : P0 == 6 ? 1 : P0 == 9 ? 2 : 3) + (mark ? 4 : 0);
+}
+
+// Periods per lane below which an item stays on the per-candidate kernel.
+static const u64 kMarkMinPeriods = 4ull * kSeg;
 
 // Largest value a chain can produce must fit three limbs.
 static bool chain_fits(const fk_engine* e, u128 x_hi, u32 cap, bool dense) {
@@ -596,14 +670,23 @@ static fk_status expand(fk_batch* b, const fk_item* items, u64 nitems) {
       di.lo_off = (s0 == 0) ? (u64)(lo - X0) : 0;
       const bool last = s0 + U >= periods;
       di.hi_last = last ? (u64)(hi - (base + (u128)(U - 1) * M)) : M;
-      const u64 words = (U + 63) / 64;
-      u64 tc = (words * L + target_chains - 1) / target_chains;
-      tc = std::min<u64>(std::max<u64>(tc, 1), 256);
-      di.Tc = (u32)tc;
-      di.nchunk = (words + tc - 1) / tc;
-      const u64 chains = di.nchunk * L;
-      di.ntask = (chains + kBlock - 1) / kBlock;
-      Family& f = b->fam[fam_of(e->P0)];
+      const bool mark = e->use_mark && (U >= kMarkMinPeriods || e->force_mark);
+      di.marked = mark ? 1 : 0;
+      if (mark) {
+        di.nchunk_u = (U + (u64)kSeg * kSegPerTask - 1) / ((u64)kSeg * kSegPerTask);
+        di.ntask = L * di.nchunk_u;
+        di.Tc = 0;
+        di.nchunk = 0;
+      } else {
+        const u64 words = (U + 63) / 64;
+        u64 tc = (words * L + target_chains - 1) / target_chains;
+        tc = std::min<u64>(std::max<u64>(tc, 1), 256);
+        di.Tc = (u32)tc;
+        di.nchunk = (words + tc - 1) / tc;
+        const u64 chains = di.nchunk * L;
+        di.ntask = (chains + kBlock - 1) / kBlock;
+      }
+      Family& f = b->fam[fam_of(e->P0, mark)];
       di.task0 = f.prefix.back();
       f.prefix.push_back(f.prefix.back() + di.ntask);
       f.idx.push_back((u32)b->items.size());
@@ -663,26 +746,34 @@ static fk_status expand(fk_batch* b, const fk_item* items, u64 nitems) {
 
 // Enqueue the whole pipeline on the batch stream (graph-capturable: no
 // host synchronisation, every size it needs is already on the device).
-static fk_status enqueue(fk_batch* b) {
+static cudaError_t record(cudaEvent_t ev, cudaStream_t s, bool capturing) {
+  return capturing ? cudaEventRecordWithFlags(ev, s, cudaEventRecordExternal)
+                   : cudaEventRecord(ev, s);
+}
+
+static fk_status enqueue(fk_batch* b, bool capturing = false) {
   cudaStream_t s = b->stream;
   const u32 ni = (u32)b->items.size();
   FK_CUDA(cudaMemsetAsync(b->d_ctr, 0, sizeof(DevCounters), s));
-  FK_CUDA(cudaMemsetAsync(b->d_task_ctr.p, 0, 4 * sizeof(unsigned long long), s));
+  FK_CUDA(cudaMemsetAsync(b->d_task_ctr.p, 0, 8 * sizeof(unsigned long long), s));
   FK_CUDA(cudaMemsetAsync(b->d_item_count.p, 0, (ni + 1) * sizeof(u32), s));
   FK_CUDA(cudaMemsetAsync(b->d_item_fill.p, 0, (ni + 1) * sizeof(u32), s));
-  FK_CUDA(cudaEventRecord(b->ev[0], s));
+  FK_CUDA(record(b->ev[0], s, capturing));
+  u64 nl = 4;  // classify, scan, scatter, sort
   if (!b->sieve_idx.empty()) {
+    ++nl;
     dim3 g(64, (u32)std::min<size_t>(b->sieve_idx.size(), 65535));
     k_xq<<<g, kBlock, 0, s>>>(b->d_engines, b->d_items.p, b->d_sieve.p,
                               (u32)b->sieve_idx.size(), b->d_xq.p);
   }
   if (!b->dense_idx.empty()) {
+    ++nl;
     k_dense<<<b->nsm * 4, kBlock, 0, s>>>(b->d_items.p, b->d_dense.p,
                                           (u32)b->dense_idx.size(),
                                           b->d_cand_key.p, b->d_cand_item.p,
                                           b->cand_cap, b->d_ctr);
   }
-  for (int f = 0; f < 4; ++f) {
+  for (int f = 0; f < 8; ++f) {
     Family& F = b->fam[f];
     if (F.idx.empty()) continue;
     SieveArgs a{};
@@ -699,17 +790,28 @@ static fk_status enqueue(fk_batch* b) {
     a.ctr = b->d_ctr;
     a.task_ctr = b->d_task_ctr.p + f;
     const u64 grid = std::min<u64>(a.ntask, (u64)b->nsm * kOccupancy);
+    ++nl;
     const u32 P0 = F.P0;
-    const size_t sm = pat_bytes_for(P0) + sizeof(SieveSmem);
-    switch (P0) {
-      case 3: k_sieve<3><<<(u32)grid, kBlock, sm, s>>>(a); break;
-      case 6: k_sieve<6><<<(u32)grid, kBlock, sm, s>>>(a); break;
-      case 9: k_sieve<9><<<(u32)grid, kBlock, sm, s>>>(a); break;
-      default: k_sieve<12><<<(u32)grid, kBlock, sm, s>>>(a); break;
+    if (F.mark) {
+      const size_t sm = pat_bytes_for(P0) + sizeof(MarkSmem);
+      switch (P0) {
+        case 3: k_mark<3><<<(u32)grid, kBlock, sm, s>>>(a); break;
+        case 6: k_mark<6><<<(u32)grid, kBlock, sm, s>>>(a); break;
+        case 9: k_mark<9><<<(u32)grid, kBlock, sm, s>>>(a); break;
+        default: k_mark<12><<<(u32)grid, kBlock, sm, s>>>(a); break;
+      }
+    } else {
+      const size_t sm = pat_bytes_for(P0) + sizeof(SieveSmem);
+      switch (P0) {
+        case 3: k_sieve<3><<<(u32)grid, kBlock, sm, s>>>(a); break;
+        case 6: k_sieve<6><<<(u32)grid, kBlock, sm, s>>>(a); break;
+        case 9: k_sieve<9><<<(u32)grid, kBlock, sm, s>>>(a); break;
+        default: k_sieve<12><<<(u32)grid, kBlock, sm, s>>>(a); break;
+      }
     }
   }
   FK_CUDA(cudaGetLastError());
-  FK_CUDA(cudaEventRecord(b->ev[1], s));
+  FK_CUDA(record(b->ev[1], s, capturing));
   ClassArgs c{};
   c.engines = b->d_engines;
   c.items = b->d_items.p;
@@ -721,7 +823,7 @@ static fk_status enqueue(fk_batch* b) {
   c.out_cap = b->out_cap;
   c.item_count = b->d_item_count.p;
   k_classify<<<b->nsm * 8, kBlock, 0, s>>>(c);
-  FK_CUDA(cudaEventRecord(b->ev[2], s));
+  FK_CUDA(record(b->ev[2], s, capturing));
   k_scan<<<1, kBlock, 0, s>>>(b->d_item_count.p, ni, b->d_item_off.p);
   k_scatter<<<b->nsm * 2, kBlock, 0, s>>>(b->d_out.p, b->d_ctr, b->out_cap,
                                           b->d_item_off.p, b->d_item_fill.p,
@@ -729,17 +831,22 @@ static fk_status enqueue(fk_batch* b) {
   k_sort_seg<<<(u32)std::min<u64>(std::max<u32>(ni, 1), (u64)b->nsm * 4), kBlock, 0, s>>>(
       b->d_sorted.p, b->d_item_off.p, b->d_nitems.p, b->d_scratch.p);
   FK_CUDA(cudaGetLastError());
-  FK_CUDA(cudaEventRecord(b->ev[3], s));
+  FK_CUDA(record(b->ev[3], s, capturing));
   FK_CUDA(cudaMemcpyAsync(b->h_ctr.p, b->d_ctr, sizeof(DevCounters),
                           cudaMemcpyDeviceToHost, s));
   FK_CUDA(cudaMemcpyAsync(b->h_off.p, b->d_item_off.p, (ni + 1) * sizeof(u64),
                           cudaMemcpyDeviceToHost, s));
+  b->last_launches = nl;
   return FK_OK;
 }
 
 static fk_status upload_items(fk_batch* b) {
   cudaStream_t s = b->stream;
   const u64 ni = b->items.size();
+  b->h2d = ni * sizeof(DevItem) + 4 * (b->dense_idx.size() +
+                                       b->sieve_idx.size() + 1);
+  for (auto& f : b->fam)
+    if (!f.idx.empty()) b->h2d += 4 * f.idx.size() + 8 * f.prefix.size();
   std::copy(b->items.begin(), b->items.end(), b->h_items.p);
   FK_CUDA(cudaMemcpyAsync(b->d_items.p, b->h_items.p, ni * sizeof(DevItem),
                           cudaMemcpyHostToDevice, s));
@@ -788,7 +895,7 @@ static fk_status launch(fk_batch* b, int use_graph) {
     if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
     if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
     FK_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    fk_status st = enqueue(b);
+    fk_status st = enqueue(b, true);
     cudaGraph_t g = nullptr;
     cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
     if (st) { if (g) cudaGraphDestroy(g); return st; }
@@ -825,6 +932,7 @@ static fk_status collect(fk_batch* b) {
   }
   const u64 ni = b->items.size();
   const u64 nout = b->h_off.p[ni];
+  b->d2h = sizeof(DevCounters) + (ni + 1) * 8 + nout * 8;
   fk_status st;
   if ((st = b->h_sorted.ensure(nout + 1))) return st;
   if (nout) {
@@ -908,6 +1016,8 @@ fk_status fk_engine_info(const fk_engine* e, fk_info* out) {
   out->first_prime = first_sieve_prime(e);
   out->nrounds = e->dev.nrounds;
   out->device_bytes = e->device_bytes;
+  out->use_mark = e->use_mark ? 1 : 0;
+  out->marked_primes = e->dev.NPm > (u32)kNS ? e->dev.NPm - kNS : 0;
   return FK_OK;
 }
 
@@ -1007,6 +1117,15 @@ fk_status fk_batch_wait(fk_batch* b, fk_batch_result* out) {
   return FK_OK;
 }
 
+fk_status fk_batch_ready(fk_batch* b, int* ready) {
+  if (!b || !ready) return set_err(FK_ERR_ARG, "null argument");
+  if (!b->pending) { *ready = 1; return FK_OK; }
+  const cudaError_t q = cudaStreamQuery(b->stream);
+  if (q == cudaSuccess) { *ready = 1; return FK_OK; }
+  if (q == cudaErrorNotReady) { *ready = 0; return FK_OK; }
+  return set_err(FK_ERR_DEVICE, cudaGetErrorString(q));
+}
+
 fk_status fk_batch_last_ms(const fk_batch* b, float* sieve_ms,
                            float* classify_ms, float* total_ms) {
   if (!b) return set_err(FK_ERR_ARG, "null argument");
@@ -1020,14 +1139,125 @@ fk_status fk_batch_last_ms(const fk_batch* b, float* sieve_ms,
   return FK_OK;
 }
 
+static fk_status stats_of(const fk_batch* b, fk_stats* out) {
+  if (!b || !out) return set_err(FK_ERR_ARG, "null argument");
+  std::memset(out, 0, sizeof(*out));
+  const DevCounters c = *b->h_ctr.p;
+  out->launches = b->last_launches;
+  out->items = b->items.size();
+  out->candidates = c.ncand;
+  out->outputs = c.nout;
+  out->s1_words = c.s1_words;
+  out->s2_tests = c.s2_tests;
+  out->imad_alg = c.imad_alg;
+  out->sprp_values = c.sprp_values;
+  out->marks = c.marks;
+  out->h2d_bytes = b->h2d;
+  out->d2h_bytes = b->d2h;
+  float a = 0, cl = 0, t = 0;
+  FK_CUDA(cudaEventElapsedTime(&a, b->ev[0], b->ev[1]));
+  FK_CUDA(cudaEventElapsedTime(&cl, b->ev[1], b->ev[2]));
+  FK_CUDA(cudaEventElapsedTime(&t, b->ev[0], b->ev[3]));
+  out->sieve_ms = a;
+  out->classify_ms = cl;
+  out->total_ms = t;
+  return FK_OK;
+}
+
+fk_status fk_batch_stats(const fk_batch* b, fk_stats* out) {
+  return stats_of(b, out);
+}
+
+fk_status fk_engine_stats(const fk_engine* e, fk_stats* out) {
+  if (!e) return set_err(FK_ERR_ARG, "null argument");
+  return stats_of(e->plain, out);
+}
+
+fk_status fk_set_device(int device) {
+  FK_CUDA(cudaSetDevice(device));
+  return FK_OK;
+}
+
 }  // extern "C"
+
+// ------------------------------------------------------- peak probes ---
+// 32-bit multiply-add throughput: 8 independent lo/hi chains per thread.
+__global__ void k_peak_imad(u32 seed, u32 iters, u32* sink) {
+  u32 x[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) x[i] = seed + threadIdx.x * 8 + i;
+  const u32 a = seed | 1u, c = seed ^ 0x9e3779b9u;
+  for (u32 it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int i = 0; i < 8; i += 2) {
+      asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(x[i]) : "r"(a), "r"(c));
+      asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(x[i + 1]) : "r"(a), "r"(c));
+    }
+  }
+  u32 r = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) r ^= x[i];
+  if (r == 0x12345678u) sink[0] = r;
+}
+
+// Shared-memory load bandwidth: each thread walks its own bank column.
+__global__ void k_peak_smem(u32 iters, u64* sink) {
+  __shared__ u64 buf[kBlock * 16];
+  for (int i = threadIdx.x; i < kBlock * 16; i += blockDim.x) buf[i] = i * 0x9e37ull;
+  __syncthreads();
+  u64 acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
+  u32 idx = threadIdx.x;
+  for (u32 it = 0; it < iters; ++it) {
+    acc0 ^= buf[idx];
+    acc1 ^= buf[idx + kBlock];
+    acc2 ^= buf[idx + 2 * kBlock];
+    acc3 ^= buf[idx + 3 * kBlock];
+    idx = (idx + 4 * kBlock) & (kBlock * 16 - 1);
+  }
+  if ((acc0 ^ acc1 ^ acc2 ^ acc3) == 0x1234ull) sink[0] = acc0;
+}
+
+extern "C" fk_status fk_peak(int which, double* per_second) {
+  if (!per_second) return set_err(FK_ERR_ARG, "null argument");
+  int dev = 0, nsm = 0;
+  FK_CUDA(cudaGetDevice(&dev));
+  FK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  void* sink = nullptr;
+  FK_CUDA(cudaMalloc(&sink, 64));
+  cudaEvent_t e0, e1;
+  FK_CUDA(cudaEventCreate(&e0));
+  FK_CUDA(cudaEventCreate(&e1));
+  const u32 grid = nsm * 8, iters = which == 0 ? 1u << 16 : 1u << 14;
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    FK_CUDA(cudaEventRecord(e0));
+    if (which == 0)
+      k_peak_imad<<<grid, kBlock>>>(rep + 7, iters, (u32*)sink);
+    else
+      k_peak_smem<<<grid, kBlock>>>(iters, (u64*)sink);
+    FK_CUDA(cudaEventRecord(e1));
+    FK_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    FK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (rep > 0) best = std::min(best, ms);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
+  const double threads = (double)grid * kBlock;
+  const double work = which == 0 ? threads * iters * 8.0        // IMADs
+                                 : threads * iters * 4.0 * 8.0; // bytes
+  *per_second = work / (best * 1e-3);
+  return FK_OK;
+}
 
 // ---------------------------------------------------- explicit values ---
 __global__ void k_sprp_vals(const u64* v, u64 n, int base2, uint8_t* out) {
   for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (u64)gridDim.x * blockDim.x) {
     V3 x = {{v[3 * i], v[3 * i + 1], v[3 * i + 2]}};
-    out[i] = sprp(x, base2 != 0) ? 1 : 0;
+    u64 im = 0;
+    out[i] = sprp(x, base2 != 0, &im) ? 1 : 0;
   }
 }
 
@@ -1037,22 +1267,23 @@ __global__ void k_depth_vals(DevEngine e, const u64* x, u64 n, u32 cap,
        i += (u64)gridDim.x * blockDim.x) {
     const u128 v = ((u128)x[2 * i + 1] << 64) | x[2 * i];
     u32 depth = 0;
+    u64 im = 0;
     if (e.kind == KIND_EULER) {
-      depth = euler_first_fail(v, cap);
+      depth = euler_first_fail(v, cap, &im);
     } else if (e.kind == KIND_DICKSON) {
       bool of = false;
       const V3 kk = v3_mul_128(v, v, &of);
       if (e.two_pass) {
-        depth = dickson_run(kk, cap, true);
-        if (depth >= 5) depth = dickson_run(kk, cap, false);
+        depth = dickson_run(kk, cap, true, &im);
+        if (depth >= 5) depth = dickson_run(kk, cap, false, &im);
       } else {
-        depth = dickson_run(kk, cap, false);
+        depth = dickson_run(kk, cap, false, &im);
       }
       if (of) depth = 255;
     } else {
       const V3 d = {{e.d_lo, e.d_hi, 0}};
-      depth = ap_run(v, d, cap, true);
-      if (depth >= 6) depth = ap_run(v, d, cap, false);
+      depth = ap_run(v, d, cap, true, &im);
+      if (depth >= 6) depth = ap_run(v, d, cap, false, &im);
     }
     out[i] = (uint8_t)min(depth, 255u);
   }

@@ -165,7 +165,8 @@ __host__ __device__ constexpr u32 pat_bytes() {
 // survivors to the global candidate list.
 template <int KIND>
 __device__ void drain(SieveSmem& S, u32 n, const DevEngine& e,
-                      const DevItem& it, u32 gitem, const SieveArgs& a) {
+                      const DevItem& it, u32 gitem, const SieveArgs& a,
+                      u64& ntest) {
   u32* qin = S.qa;
   u32* qout = S.qb;
   const u32* __restrict__ xq = a.xq + it.xq_off;
@@ -181,7 +182,8 @@ __device__ void drain(SieveSmem& S, u32 n, const DevEngine& e,
                     (code & 63u);
       const u64 v = u * M + S.chain_R[t];
       bool alive = true;
-      for (u32 i = i0; i < i1; ++i) {
+      u32 i = i0;
+      for (; i < i1; ++i) {
         const PrimeRec pr = e.recs[i];
         u32 rr = fk_bmod(v, pr.q, pr.magic) + __ldg(xq + i);
         rr = min(rr, rr - pr.q);
@@ -190,6 +192,7 @@ __device__ void drain(SieveSmem& S, u32 n, const DevEngine& e,
           break;
         }
       }
+      ntest += (i - i0) + (alive ? 0 : 1);
       mask |= (u32)alive << k;
     }
     u32 tot;
@@ -321,11 +324,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_sieve(SieveArgs a) {
     Pat<P0, 0, kNS>::setup(rho, R, 64ull * w0, a.xq + it.xq_off, S.minv);
     const u64 U = it.U;
     u32 qn = 0;
+    u64 ntest = 0, nword = 0;
     __syncthreads();
     for (u32 wi = 0; wi < it.Tc; ++wi) {
       const u64 w = w0 + wi;
       u64 surv = 0;
       if (active && 64ull * w < U) {
+        ++nword;
         u64 acc = 0;
         Pat<P0, 0, kNS>::word(spat, rho, acc);
         const u64 left = U - 64ull * w;
@@ -363,18 +368,27 @@ __global__ void __launch_bounds__(kBlock, 2) k_sieve(SieveArgs a) {
         }
         __syncthreads();
         switch (e.kind) {
-          case KIND_EULER: drain<KIND_EULER>(S, qn, e, it, gitem, a); break;
-          case KIND_DICKSON: drain<KIND_DICKSON>(S, qn, e, it, gitem, a); break;
-          default: drain<KIND_AP>(S, qn, e, it, gitem, a); break;
+          case KIND_EULER: drain<KIND_EULER>(S, qn, e, it, gitem, a, ntest); break;
+          case KIND_DICKSON: drain<KIND_DICKSON>(S, qn, e, it, gitem, a, ntest); break;
+          default: drain<KIND_AP>(S, qn, e, it, gitem, a, ntest); break;
         }
         qn = 0;
       }
       __syncthreads();
     }
     switch (e.kind) {
-      case KIND_EULER: drain<KIND_EULER>(S, qn, e, it, gitem, a); break;
-      case KIND_DICKSON: drain<KIND_DICKSON>(S, qn, e, it, gitem, a); break;
-      default: drain<KIND_AP>(S, qn, e, it, gitem, a); break;
+      case KIND_EULER: drain<KIND_EULER>(S, qn, e, it, gitem, a, ntest); break;
+      case KIND_DICKSON: drain<KIND_DICKSON>(S, qn, e, it, gitem, a, ntest); break;
+      default: drain<KIND_AP>(S, qn, e, it, gitem, a, ntest); break;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ntest += __shfl_down_sync(0xffffffffu, ntest, o);
+      nword += __shfl_down_sync(0xffffffffu, nword, o);
+    }
+    if ((tid & 31) == 0) {
+      if (ntest) atomicAdd(&a.ctr->s2_tests, (unsigned long long)ntest);
+      if (nword) atomicAdd(&a.ctr->s1_words, (unsigned long long)nword);
     }
   }
 }

@@ -179,7 +179,7 @@ __device__ __forceinline__ u32 small_mod(const u64* m, u32 s, u32 c) {
 // huntlib/primes.py:23-80 for an L-limb m whose top limb is nonzero.
 // nbases = 7 gives mr_is_prime, nbases = 1 gives sprp_base2.
 template <int L>
-__device__ bool sprp_L(const u64* m, int nbases) {
+__device__ bool sprp_L(const u64* m, int nbases, u64* imad) {
   if (L == 1 && m[0] < 2) return false;
   // trial division by 2..37 via two composite moduli
   // 223092870 = 2*3*5*7*11*13*17*19*23 ; 33263 = 29*31*37
@@ -246,6 +246,10 @@ __device__ bool sprp_L(const u64* m, int nbases) {
   for (int i = L - 1; i >= 0; --i)
     if (d[i] && dtop == 0) dtop = 64 * i + 63 - __clzll(d[i]);
 
+  // algorithmic work of one strong test (32-bit CIOS): (bits - 1) squarings
+  // of 2l^2 + l word products, each a lo and a hi multiply-add
+  const u64 l32 = (u64)((bl + 31) >> 5);
+  const u64 per_base = (u64)(bl - 1) * (4 * l32 * l32 + 2 * l32);
   for (int bi = 0; bi < nbases; ++bi) {
     u64 a = kMrBases[bi];
     if (L == 1 && m[0] <= a) {
@@ -256,6 +260,7 @@ __device__ bool sprp_L(const u64* m, int nbases) {
 #pragma unroll
     for (int i = 0; i < L; ++i) av[i] = 0;
     av[0] = a;
+    *imad += per_base;
     mont_mul<L>(at, av, r2m, m, minv);  // a * R mod m
 #pragma unroll
     for (int i = 0; i < L; ++i) x[i] = at[i];
@@ -274,12 +279,13 @@ __device__ bool sprp_L(const u64* m, int nbases) {
   return true;
 }
 
-// Dispatch on the limb count of v.  base2_only selects sprp_base2.
-__device__ __noinline__ bool sprp(const V3& v, bool base2_only) {
+// Dispatch on the limb count of v.  base2_only selects sprp_base2.  *imad
+// accumulates the algorithmic multiply-add count of the bases run.
+__device__ __noinline__ bool sprp(const V3& v, bool base2_only, u64* imad) {
   const int nb = base2_only ? 1 : 7;
-  if (v.w[2]) return sprp_L<3>(v.w, nb);
-  if (v.w[1]) return sprp_L<2>(v.w, nb);
-  return sprp_L<1>(v.w, nb);
+  if (v.w[2]) return sprp_L<3>(v.w, nb, imad);
+  if (v.w[1]) return sprp_L<2>(v.w, nb, imad);
+  return sprp_L<1>(v.w, nb, imad);
 }
 
 }  // namespace fk

@@ -25,6 +25,8 @@ constexpr int kQcap = 4096;       // per-CTA candidate queue (entries)
 constexpr int kNS = 32;           // pattern primes per chain
 constexpr int kMaxRounds = 64;
 constexpr int kSortSmem = 4096;   // entries a CTA sorts in shared memory
+constexpr int kSeg = 32768;       // marking: periods per shared segment
+constexpr int kSegPerTask = 8;    // marking: segments per task
 
 // Immutable per-engine tables (device-resident for the engine's life).
 struct DevEngine {
@@ -42,6 +44,13 @@ struct DevEngine {
   const uint32_t* lists;          // explicit forbidden-residue lists
   const uint32_t* rounds;         // [nrounds + 1] prime-index cuts
   const uint32_t* sbits;          // Euler: bitset of {x^2 + x : x < n}
+  // marking sieve (long lanes): primes [NS, NPm) are marked in a per-lane
+  // byte map; G lists hold each prime's forbidden residues of the PERIOD
+  // u for lane offset 0 (f * (M mod q)^-1 mod q)
+  uint32_t NPm, use_mark;
+  const uint32_t* minv_all;       // [NP] (M mod q)^-1 mod q
+  const uint32_t* gaux;           // [NP] offset | count << 24 into glist
+  const uint32_t* glist;
 };
 
 // One unit of work: a sub-range of one engine's line.
@@ -55,6 +64,8 @@ struct DevItem {
   uint64_t nchunk;                // chains per lane
   uint64_t task0, ntask;          // first task, task count
   uint64_t xq_off;                // this item's base-residue table
+  uint32_t marked, pad2;          // 1: the marking kernel sweeps this item
+  uint64_t nchunk_u;              // marking: u-chunks per lane
 };
 
 // Output entry before ordering: item index + (key << 8 | depth).
@@ -68,8 +79,14 @@ struct DevCounters {
   unsigned long long task_next;   // persistent task counter
   unsigned long long ncand;       // candidates written
   unsigned long long nout;        // outputs written
-  unsigned int overflow;          // bit 0 cand, bit 1 out, bit 2 timeout
+  unsigned int overflow;          // bit 0 cand, bit 1 out, bit 2 timeout,
+                                  // bit 3 value past 192 bits
   unsigned int pad;
+  unsigned long long s1_words;    // pattern-sieve words processed
+  unsigned long long s2_tests;    // per-candidate prime tests
+  unsigned long long imad_alg;    // algorithmic IMADs of the SPRP stage
+  unsigned long long sprp_values; // values strong-tested
+  unsigned long long marks;       // marking-sieve byte marks
 };
 
 }  // namespace fk

@@ -32,13 +32,14 @@ _u32 = ctypes.c_uint32
 class Params(ctypes.Structure):
     _fields_ = [("kind", _u32), ("n", _u32), ("q2", _u32), ("p0", _u32),
                 ("d_lo", _u64), ("d_hi", _u64), ("two_pass", _u32),
-                ("reserved", _u32)]
+                ("sieve", _u32)]
 
 
 class Info(ctypes.Structure):
     _fields_ = [("M", _u64), ("W", _u64), ("L", _u32), ("NP", _u32),
                 ("first_prime", _u32), ("nrounds", _u32),
-                ("device_bytes", _u64)]
+                ("device_bytes", _u64), ("use_mark", _u32),
+                ("marked_primes", _u32)]
 
 
 class Result(ctypes.Structure):
@@ -49,6 +50,18 @@ class Result(ctypes.Structure):
 class Item(ctypes.Structure):
     _fields_ = [("engine", _u32), ("mode", _u32), ("threshold", _u32),
                 ("cap", _u32), ("lo", _u64 * 2), ("hi", _u64 * 2)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("launches", _u64), ("items", _u64), ("candidates", _u64),
+                ("outputs", _u64), ("s1_words", _u64), ("s2_tests", _u64),
+                ("imad_alg", _u64), ("sprp_values", _u64),
+                ("marks", _u64), ("h2d_bytes", _u64), ("d2h_bytes", _u64),
+                ("sieve_ms", ctypes.c_float), ("classify_ms", ctypes.c_float),
+                ("total_ms", ctypes.c_float), ("pad", _u32)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_ if f != "pad"}
 
 
 class BatchResult(ctypes.Structure):
@@ -90,10 +103,19 @@ SIGNATURES = {
                                          ctypes.c_int]),
     "fk_batch_wait": (ctypes.c_int32, [ctypes.c_void_p,
                                        ctypes.POINTER(BatchResult)]),
+    "fk_batch_ready": (ctypes.c_int32, [ctypes.c_void_p,
+                                        ctypes.POINTER(ctypes.c_int)]),
     "fk_batch_last_ms": (ctypes.c_int32, [ctypes.c_void_p,
                                           ctypes.POINTER(ctypes.c_float),
                                           ctypes.POINTER(ctypes.c_float),
                                           ctypes.POINTER(ctypes.c_float)]),
+    "fk_batch_stats": (ctypes.c_int32, [ctypes.c_void_p,
+                                        ctypes.POINTER(Stats)]),
+    "fk_engine_stats": (ctypes.c_int32, [ctypes.c_void_p,
+                                         ctypes.POINTER(Stats)]),
+    "fk_set_device": (ctypes.c_int32, [ctypes.c_int]),
+    "fk_peak": (ctypes.c_int32, [ctypes.c_int,
+                                 ctypes.POINTER(ctypes.c_double)]),
     "fk_last_error": (ctypes.c_char_p, []),
     "fk_sprp": (ctypes.c_int32, [ctypes.POINTER(_u64), _u64, ctypes.c_int,
                                  ctypes.POINTER(ctypes.c_uint8)]),
@@ -149,9 +171,13 @@ def _arrays(res):
 class Engine:
     """One device engine: wheel, pattern tables, kill tests, rounds."""
 
-    def __init__(self, kind, n, q2=65536, p0=0, d=None, two_pass=False):
+    def __init__(self, kind, n, q2=65536, p0=0, d=None, two_pass=False,
+                 sieve=None):
         lib = load()
         p = Params()
+        if sieve is None:
+            sieve = os.environ.get("FK_SIEVE", "auto")
+        p.sieve = {"auto": 0, "rounds": 1, "mark": 2}[sieve]
         p.kind, p.n, p.q2, p.p0 = int(kind), int(n), int(q2), int(p0)
         dd = int(d or 0)
         p.d_lo, p.d_hi = dd & (2 ** 64 - 1), dd >> 64
@@ -167,6 +193,8 @@ class Engine:
         self.NP, self.first_prime = int(inf.NP), int(inf.first_prime)
         self.nrounds = int(inf.nrounds)
         self.device_bytes = int(inf.device_bytes)
+        self.use_mark = bool(inf.use_mark)
+        self.marked_primes = int(inf.marked_primes)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -203,6 +231,11 @@ class Engine:
         _check(self._lib.fk_dense(self._h, u128(lo), u128(hi),
                                   int(threshold), int(cap), ctypes.byref(r)))
         return _arrays(r)
+
+    def stats(self):
+        st = Stats()
+        _check(self._lib.fk_engine_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
 
     def depths(self, xs, cap):
         """Chain depth of each explicit chain start in xs."""
@@ -287,10 +320,20 @@ class Batch:
         _check(self._lib.fk_batch_submit(self._h, arr, len(specs),
                                          1 if graph else 0))
 
+    def ready(self):
+        r = ctypes.c_int()
+        _check(self._lib.fk_batch_ready(self._h, ctypes.byref(r)))
+        return bool(r.value)
+
     def wait(self):
         br = BatchResult()
         _check(self._lib.fk_batch_wait(self._h, ctypes.byref(br)))
         return self._unpack(br)
+
+    def stats(self):
+        st = Stats()
+        _check(self._lib.fk_batch_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
 
     def last_ms(self):
         a, c, t = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
@@ -323,6 +366,19 @@ def sprp(values, base2_only=False):
 
 def version():
     return load().fk_version().decode()
+
+
+def set_device(device):
+    """Point libfk's runtime at a CUDA device for this host thread."""
+    _check(load().fk_set_device(int(device)))
+
+
+def peak(which):
+    """Measured peak: 'imad' -> 32-bit multiply-adds/s, 'smem' -> shared
+    load bytes/s."""
+    out = ctypes.c_double()
+    _check(load().fk_peak({"imad": 0, "smem": 1}[which], ctypes.byref(out)))
+    return float(out.value)
 
 
 def device_count():

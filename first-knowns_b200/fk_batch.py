@@ -1,0 +1,139 @@
+"""The persistent batched engine and its plain per-interval counterpart.
+
+``BatchEngine`` keeps one device engine per (kind, n, q2, d) -- wheel,
+pattern, prime and kill-test tables stay resident across runs -- and
+sweeps any number of intervals of mixed engine type in ONE pipeline: a
+persistent sieve grid pulls (interval, chain block) tasks from a device
+counter, the SPRP stage classifies every survivor, and the stream comes
+back ordered per interval.  With ``graph=True`` the pipeline is a
+captured CUDA graph, replayed while the batch shape is unchanged.
+
+``PlainEngine`` runs the same intervals one at a time through each
+engine's own per-interval call (fk_hunt): the baseline the batch is
+measured against.  Both return identical results by construction; the
+tests check it.
+"""
+
+import fk_abi
+from fk_workloads import (AP, DICKSON, EULER, engine_key, line_range,
+                          rows_to_results)
+
+
+def _p0_for(kind, n):
+    # one pattern family for every engine in a batch (see the sieve
+    # kernel's compile-time pattern primes); 17 is the first pattern prime
+    return 6
+
+
+class EngineSet:
+    """Device engines keyed by (kind, n, q2, d), created on first use."""
+
+    def __init__(self):
+        self._engines = {}
+        self._order = []
+
+    def get(self, key):
+        if key not in self._engines:
+            kind, n, q2, d = key
+            self._engines[key] = fk_abi.Engine(kind, n, q2=q2,
+                                               p0=_p0_for(kind, n),
+                                               d=d or None)
+            self._order.append(key)
+        return self._engines[key]
+
+    def index(self, key):
+        self.get(key)
+        return self._order.index(key)
+
+    def engines(self):
+        return [self._engines[k] for k in self._order]
+
+    def device_bytes(self):
+        return sum(e.device_bytes for e in self._engines.values())
+
+
+def item_specs(engset, intervals):
+    """fk_item specs (engine index, mode, threshold, cap, lo, hi)."""
+    specs = []
+    for iv in intervals:
+        key = engine_key(iv)
+        e = engset.get(key)
+        lo, hi = line_range(iv, e.W if iv.kind == DICKSON else 1)
+        specs.append((engset.index(key), fk_abi.MODE_HUNT, iv.threshold,
+                      iv.cap, lo, hi))
+    return specs
+
+
+class BatchEngine:
+    """Sweep many intervals in one persistent launch."""
+
+    def __init__(self, intervals=(), engset=None):
+        self.engset = engset or EngineSet()
+        for iv in intervals:
+            self.engset.get(engine_key(iv))
+        self._batch = None
+        self._nengines = -1
+
+    def _ensure(self):
+        n = len(self.engset.engines())
+        if self._batch is None or n != self._nengines:
+            if self._batch is not None:
+                self._batch.close()
+            self._batch = fk_abi.Batch(self.engset.engines())
+            self._nengines = n
+        return self._batch
+
+    def run(self, intervals, graph=True):
+        """[(x, depth)] per interval, ascending, depth >= threshold."""
+        specs = item_specs(self.engset, intervals)
+        b = self._ensure()
+        rows = b.run(specs, graph=graph)
+        out = []
+        for iv, (off, dep) in zip(intervals, rows):
+            e = self.engset.get(engine_key(iv))
+            out.append(rows_to_results(iv, off, dep,
+                                       e.W if iv.kind == DICKSON else 1))
+        return out
+
+    def submit(self, intervals, graph=False):
+        specs = item_specs(self.engset, intervals)
+        self._pending = list(intervals)
+        self._ensure().submit(specs, graph=graph)
+
+    def wait(self):
+        rows = self._batch.wait()
+        out = []
+        for iv, (off, dep) in zip(self._pending, rows):
+            e = self.engset.get(engine_key(iv))
+            out.append(rows_to_results(iv, off, dep,
+                                       e.W if iv.kind == DICKSON else 1))
+        return out
+
+    def last_ms(self):
+        """(sieve, classify, whole pipeline) device ms of the last run."""
+        return self._batch.last_ms()
+
+    def stats(self):
+        """Device work counters and event times of the last run."""
+        return self._batch.stats()
+
+
+class PlainEngine:
+    """The same intervals, one fk_hunt call each."""
+
+    def __init__(self, engset=None):
+        self.engset = engset or EngineSet()
+
+    def run(self, intervals):
+        out = []
+        for iv in intervals:
+            e = self.engset.get(engine_key(iv))
+            W = e.W if iv.kind == DICKSON else 1
+            lo, hi = line_range(iv, W)
+            off, dep = e.hunt(lo, hi, iv.threshold, iv.cap)
+            out.append(rows_to_results(iv, off, dep, W))
+        return out
+
+
+__all__ = ["BatchEngine", "PlainEngine", "EngineSet", "EULER", "DICKSON",
+           "AP"]

@@ -51,7 +51,8 @@ typedef struct fk_params {
                        * wheel); 0 picks a default for the kind               */
   uint64_t d_lo, d_hi;/* AP difference (0, 0: the n-th primorial)             */
   uint32_t two_pass;  /* Dickson: launcher's two-pass sprp_run depth          */
-  uint32_t reserved;
+  uint32_t sieve;     /* 0 auto (cost model + lane length), 1 compaction      *
+                       * rounds only, 2 marking sieve for every item          */
 } fk_params;
 
 /* Read-only description of an engine, for the Python mirrors. */
@@ -63,6 +64,8 @@ typedef struct fk_info {
   uint32_t first_prime;/* smallest sieve prime not folded into the wheel      */
   uint32_t nrounds;    /* compaction rounds                                   */
   uint64_t device_bytes; /* bytes this engine holds on the device             */
+  uint32_t use_mark;   /* long lanes use the marking sieve (cost model)      */
+  uint32_t marked_primes; /* primes the marking sieve covers                 */
 } fk_info;
 
 /* One ordered result: x = base + offset[i]; depth[i] is the chain depth
@@ -139,9 +142,34 @@ fk_status fk_batch_run(fk_batch* b, const fk_item* items, uint64_t nitems,
 fk_status fk_batch_submit(fk_batch* b, const fk_item* items, uint64_t nitems,
                           int use_graph);
 fk_status fk_batch_wait(fk_batch* b, fk_batch_result* out);
+/* Non-blocking: *ready = 1 once a submitted run has finished on the
+ * device (fk_batch_wait then returns without waiting on the GPU). */
+fk_status fk_batch_ready(fk_batch* b, int* ready);
 /* Device time (ms) of the last run's kernels, from CUDA events. */
 fk_status fk_batch_last_ms(const fk_batch* b, float* sieve_ms,
                            float* classify_ms, float* total_ms);
+
+/* Counters of the last run (device-side work accounting). */
+typedef struct fk_stats {
+  uint64_t launches;     /* kernels launched by the run                      */
+  uint64_t items;        /* device items (launch-sized sub-ranges)          */
+  uint64_t candidates;   /* pre-primality survivors (or dense values)       */
+  uint64_t outputs;      /* ordered entries returned                        */
+  uint64_t s1_words;     /* 64-candidate words the pattern sieve processed  */
+  uint64_t s2_tests;     /* per-candidate prime tests in the rounds         */
+  uint64_t imad_alg;     /* algorithmic 32-bit multiply-adds of the SPRP    *
+                          * stage: (bits(N)-1)*(4l^2+2l) per strong base,   *
+                          * l = ceil(bits(N)/32)                            */
+  uint64_t sprp_values;  /* values strong-tested                            */
+  uint64_t marks;        /* byte marks of the marking sieve                 */
+  uint64_t h2d_bytes;    /* host-to-device bytes the run copied             */
+  uint64_t d2h_bytes;    /* device-to-host bytes the run copied             */
+  float sieve_ms, classify_ms, total_ms;
+  uint32_t pad;
+} fk_stats;
+fk_status fk_batch_stats(const fk_batch* b, fk_stats* out);
+/* The same counters for an engine's last plain call. */
+fk_status fk_engine_stats(const fk_engine* e, fk_stats* out);
 
 /* ---- misc -------------------------------------------------------------- */
 /* Last error message on this thread. */
@@ -152,6 +180,13 @@ fk_status fk_sprp(const uint64_t* v_limbs, uint64_t count, int base2_only,
                   uint8_t* out);
 /* Library version string. */
 const char* fk_version(void);
+/* Select the CUDA device for this host thread's later libfk calls (libfk
+ * carries its own runtime state; a caller's runtime does not set it). */
+fk_status fk_set_device(int device);
+/* Measured device peaks for the rooflines: which = 0 gives 32-bit integer
+ * multiply-adds per second (IMAD, lo and hi halves alternating), which = 1
+ * shared-memory load bytes per second (64-bit, bank-conflict free). */
+fk_status fk_peak(int which, double* per_second);
 
 #ifdef __cplusplus
 }
