@@ -42,7 +42,8 @@ def build(force=False, verbose=False):
     if not force and not needs_build():
         return LIB
     cmd = [NVCC] + FLAGS + ["-o", str(LIB) + ".tmp",
-                            str(CSRC / "fk_engine.cu")]
+                            str(CSRC / "fk_engine.cu"),
+                            str(CSRC / "fk_noalloc.cu")]
     res = subprocess.run(cmd, capture_output=True, text=True)
     log = res.stdout + res.stderr
     (HERE / "build.log").write_text(log)

@@ -16,6 +16,7 @@
 #include "../../include/fk.h"
 #include "fk_arith.cuh"
 #include "fk_classify.cuh"
+#include "fk_internal.h"
 #include "fk_mark.cuh"
 #include "fk_sieve.cuh"
 #include "fk_types.h"
@@ -1179,6 +1180,20 @@ fk_status fk_set_device(int device) {
 }
 
 }  // extern "C"
+
+namespace fk {
+EngineView engine_view(const fk_engine* e) {
+  EngineView v;
+  v.dev = e->dev;
+  v.P0 = e->P0;
+  v.M = e->M;
+  v.L = (uint32_t)e->lanes.size();
+  v.NP = (uint32_t)e->sieve.size();
+  return v;
+}
+
+fk_status set_error(fk_status s, const char* msg) { return set_err(s, msg); }
+}  // namespace fk
 
 // ------------------------------------------------------- peak probes ---
 // 32-bit multiply-add throughput: 8 independent lo/hi chains per thread.

@@ -1,0 +1,248 @@
+// fk_noalloc.cu -- fk_sieve_noalloc: the pre-primality sieve of one
+// interval for callers that cannot allocate device memory.
+//
+// Some callers cannot call cudaMalloc when they sweep: a real-time loop
+// whose memory budget is fixed up front, a host framework that owns every
+// allocation through its own pool and forbids the library from growing
+// the heap behind its back, or code that must not trigger the implicit
+// synchronisation an allocation can cause.  fk_sieve (fk_engine.cu) grows
+// its buffers on demand; this entry point instead keeps every piece of
+// per-call scratch -- the item descriptor, the base-residue table, the
+// candidate list, the counters and the sort buffer -- in one fixed array
+// in device memory, declared below, and writes its result into buffers
+// the caller owns.  It calls no cudaMalloc, cudaFree or other allocating
+// routine; the engine's own tables were uploaded when the engine was
+// created.
+//
+// Limits (rejected with FK_ERR_DOMAIN and a message before any launch):
+//   * at most kMaxPrimes sieve primes (q2 up to about 821,000);
+//   * the interval must fit one device item (periods * M below 2^55);
+// and at run time, more than kMaxCand pre-primality survivors (or more
+// than the caller's capacity) is reported by writing UINT64_MAX to the
+// caller's count instead of a result.
+//
+// Sharing: every call, from any thread, uses the same array on a given
+// device, and the array keeps the previous call's contents; each call
+// clears its counters first.  Two calls whose work overlaps on the GPU
+// (different streams, or different host threads) race on the array and
+// both results are undefined.  Serialize them, e.g. on one stream.
+//
+// Set-up: the first call on a device, with that device current, looks up
+// the array's device address (cudaGetSymbolAddress) and sets the sieve
+// kernels' shared-memory limits; make that first call before any stream
+// capture is active.  Every GPU that loads the library holds the array
+// (kScratchBytes, about 5.3 MiB) until the process exits.
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "../../include/fk.h"
+#include "fk_internal.h"
+#include "fk_sieve.cuh"
+
+using namespace fk;
+
+namespace {
+
+constexpr uint64_t kMaxCand = 1ull << 18;   // survivors one call may emit
+constexpr uint32_t kMaxPrimes = 1u << 16;   // sieve primes of the engine
+
+// byte layout of the scratch array
+constexpr size_t kOffCtr = 0;
+constexpr size_t kOffTaskCtr = 256;
+constexpr size_t kOffItem = 512;
+constexpr size_t kOffEngine = 1024;
+constexpr size_t kOffPrefix = 2048;
+constexpr size_t kOffIndex = 2304;
+constexpr size_t kOffXq = 4096;
+constexpr size_t kOffKey = kOffXq + 4ull * kMaxPrimes;
+constexpr size_t kOffCandItem = kOffKey + 8ull * kMaxCand;
+constexpr size_t kOffSort = kOffCandItem + 4ull * kMaxCand;
+constexpr size_t kScratchBytes = kOffSort + 8ull * kMaxCand;
+
+static_assert(sizeof(DevCounters) <= kOffTaskCtr - kOffCtr, "layout");
+static_assert(sizeof(DevItem) <= kOffEngine - kOffItem, "layout");
+static_assert(sizeof(DevEngine) <= kOffPrefix - kOffEngine, "layout");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+std::mutex g_setup_mu;
+unsigned char* g_scratch_addr[64] = {nullptr};
+
+template <typename T>
+T* at(unsigned char* base, size_t off) {
+  return reinterpret_cast<T*>(base + off);
+}
+
+// Writes this call's descriptors into the scratch array and zeroes its
+// counters (the array keeps the last call's contents otherwise).
+__global__ void k_na_init(unsigned char* s, DevEngine eng, DevItem item,
+                          unsigned long long ntask) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    DevCounters* c = reinterpret_cast<DevCounters*>(s + kOffCtr);
+    *c = DevCounters{};
+    *reinterpret_cast<unsigned long long*>(s + kOffTaskCtr) = 0ull;
+    *reinterpret_cast<DevItem*>(s + kOffItem) = item;
+    *reinterpret_cast<DevEngine*>(s + kOffEngine) = eng;
+    u64* pre = reinterpret_cast<u64*>(s + kOffPrefix);
+    pre[0] = 0;
+    pre[1] = ntask;
+    *reinterpret_cast<u32*>(s + kOffIndex) = 0u;
+  }
+}
+
+// X0 mod q for every sieve prime of the call's item, into the array.
+__global__ void k_na_xq(unsigned char* s) {
+  const DevItem* it = reinterpret_cast<const DevItem*>(s + kOffItem);
+  const DevEngine* e = reinterpret_cast<const DevEngine*>(s + kOffEngine);
+  u32* xq = reinterpret_cast<u32*>(s + kOffXq);
+  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < e->NP;
+       i += gridDim.x * blockDim.x) {
+    const PrimeRec pr = e->recs[i];
+    xq[i] = fk_bmod128(it->X0_lo, it->X0_hi, pr.q, pr.magic, e->c64[i]);
+  }
+}
+
+// Orders the survivors and writes them, as offsets from the caller's lo,
+// into the caller's buffer (one CTA; bitonic sort inside the array).
+__global__ void __launch_bounds__(kBlock) k_na_finish(
+    unsigned char* s, u64* out, u64 capacity, u64* count, u64 lo_shift) {
+  const DevCounters* c = reinterpret_cast<const DevCounters*>(s + kOffCtr);
+  const u64 n = c->ncand;
+  if (n > kMaxCand || n > capacity || (c->overflow & 5u)) {
+    if (threadIdx.x == 0) *count = ~0ull;
+    return;
+  }
+  const u64* key = reinterpret_cast<const u64*>(s + kOffKey);
+  u64* buf = reinterpret_cast<u64*>(s + kOffSort);
+  u32 npow = 1;
+  while (npow < n) npow <<= 1;
+  for (u32 i = threadIdx.x; i < npow; i += blockDim.x)
+    buf[i] = i < n ? key[i] : ~0ull;
+  __syncthreads();
+  for (u32 k = 2; k <= npow; k <<= 1) {
+    for (u32 j = k >> 1; j > 0; j >>= 1) {
+      for (u32 i = threadIdx.x; i < npow; i += blockDim.x) {
+        const u32 l = i ^ j;
+        if (l > i) {
+          const u64 x = buf[i], y = buf[l];
+          if ((x > y) == ((i & k) == 0)) {
+            buf[i] = y;
+            buf[l] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (u32 i = threadIdx.x; i < n; i += blockDim.x) out[i] = buf[i] - lo_shift;
+  if (threadIdx.x == 0) *count = n;
+}
+
+template <int P0>
+cudaError_t set_smem_limit() {
+  return cudaFuncSetAttribute(k_sieve<P0>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(pat_bytes<P0>() + sizeof(SieveSmem)));
+}
+
+}  // namespace
+
+extern "C" fk_status fk_sieve_noalloc(fk_engine* e, const uint64_t lo[2],
+                                      const uint64_t hi[2], uint64_t* d_offsets,
+                                      uint64_t capacity, uint64_t* d_count,
+                                      void* stream) {
+  if (!e || !lo || !hi || !d_offsets || !d_count)
+    return set_error(FK_ERR_ARG, "fk_sieve_noalloc: null argument");
+  const EngineView v = engine_view(e);
+  if (v.NP > kMaxPrimes)
+    return set_error(FK_ERR_DOMAIN,
+                     "fk_sieve_noalloc: the engine has more than 65536 sieve "
+                     "primes (q2 too deep for the fixed scratch array)");
+  const u128 L0 = ((u128)lo[1] << 64) | lo[0];
+  const u128 H0 = ((u128)hi[1] << 64) | hi[0];
+  if (H0 <= L0)
+    return set_error(FK_ERR_DOMAIN, "fk_sieve_noalloc: empty interval");
+  const u64 M = v.M;
+  const u128 X0 = L0 / M * M;
+  const u128 periods = (H0 - X0 + M - 1) / M;
+  u64 umax = (u64)(((u128)1 << 55) / M);
+  umax = umax / 64 * 64;
+  if (periods > (u128)umax || periods >= ((u128)1 << 36))
+    return set_error(FK_ERR_DOMAIN,
+                     "fk_sieve_noalloc: interval too long for one call "
+                     "(periods * M must stay below 2^55)");
+  // per-device set-up: the array's device address and kernel attributes
+  int dev = 0;
+  cudaError_t ce = cudaGetDevice(&dev);
+  if (ce != cudaSuccess) return set_error(FK_ERR_DEVICE, cudaGetErrorString(ce));
+  if (dev < 0 || dev >= 64) return set_error(FK_ERR_DEVICE, "device index above 63");
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_setup_mu);
+    if (!g_scratch_addr[dev]) {
+      void* p = nullptr;
+      ce = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (ce != cudaSuccess)
+        return set_error(FK_ERR_DEVICE, cudaGetErrorString(ce));
+      for (cudaError_t r : {set_smem_limit<3>(), set_smem_limit<6>(),
+                            set_smem_limit<9>(), set_smem_limit<12>()})
+        if (r != cudaSuccess) return set_error(FK_ERR_DEVICE, cudaGetErrorString(r));
+      g_scratch_addr[dev] = static_cast<unsigned char*>(p);
+    }
+    base = g_scratch_addr[dev];
+  }
+  int nsm = 0;
+  ce = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (ce != cudaSuccess) return set_error(FK_ERR_DEVICE, cudaGetErrorString(ce));
+  // the one device item: the same line geometry the batch pipeline uses
+  const u64 U = (u64)periods;
+  DevItem it{};
+  it.engine = 0;
+  it.mode = MODE_SIEVE;
+  it.X0_lo = (u64)X0;
+  it.X0_hi = (u64)(X0 >> 64);
+  it.U = U;
+  it.lo_off = (u64)(L0 - X0);
+  it.hi_last = (u64)(H0 - (X0 + (u128)(U - 1) * M));
+  const u64 words = (U + 63) / 64;
+  const u64 target = (u64)nsm * 2 * kBlock * 4;
+  u64 tc = (words * v.L + target - 1) / target;
+  tc = tc < 1 ? 1 : (tc > 256 ? 256 : tc);
+  it.Tc = (u32)tc;
+  it.nchunk = (words + tc - 1) / tc;
+  const u64 ntask = (it.nchunk * v.L + kBlock - 1) / kBlock;
+  it.ntask = ntask;
+  it.xq_off = 0;
+  it.marked = 0;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  k_na_init<<<1, 32, 0, s>>>(base, v.dev, it, ntask);
+  k_na_xq<<<64, kBlock, 0, s>>>(base);
+  SieveArgs a{};
+  a.engines = at<DevEngine>(base, kOffEngine);
+  a.items = at<DevItem>(base, kOffItem);
+  a.task_prefix = at<u64>(base, kOffPrefix);
+  a.item_index = at<u32>(base, kOffIndex);
+  a.nitems = 1;
+  a.ntask = ntask;
+  a.xq = at<u32>(base, kOffXq);
+  a.cand_key = at<u64>(base, kOffKey);
+  a.cand_item = at<u32>(base, kOffCandItem);
+  a.cand_cap = kMaxCand;
+  a.ctr = at<DevCounters>(base, kOffCtr);
+  a.task_ctr = at<unsigned long long>(base, kOffTaskCtr);
+  const u32 grid = (u32)(ntask < (u64)nsm * 2 ? ntask : (u64)nsm * 2);
+  switch (v.P0) {
+    case 3: k_sieve<3><<<grid, kBlock, pat_bytes<3>() + sizeof(SieveSmem), s>>>(a); break;
+    case 6: k_sieve<6><<<grid, kBlock, pat_bytes<6>() + sizeof(SieveSmem), s>>>(a); break;
+    case 9: k_sieve<9><<<grid, kBlock, pat_bytes<9>() + sizeof(SieveSmem), s>>>(a); break;
+    default: k_sieve<12><<<grid, kBlock, pat_bytes<12>() + sizeof(SieveSmem), s>>>(a); break;
+  }
+  const u64 lo_shift = (u64)(L0 - X0);
+  k_na_finish<<<1, kBlock, 0, s>>>(base, reinterpret_cast<u64*>(d_offsets),
+                                   capacity, reinterpret_cast<u64*>(d_count),
+                                   lo_shift);
+  ce = cudaGetLastError();
+  if (ce != cudaSuccess) return set_error(FK_ERR_DEVICE, cudaGetErrorString(ce));
+  return FK_OK;
+}

@@ -120,6 +120,11 @@ SIGNATURES = {
     "fk_sprp": (ctypes.c_int32, [ctypes.POINTER(_u64), _u64, ctypes.c_int,
                                  ctypes.POINTER(ctypes.c_uint8)]),
     "fk_version": (ctypes.c_char_p, []),
+    "fk_sieve_noalloc": (ctypes.c_int32, [ctypes.c_void_p,
+                                          ctypes.POINTER(_u64),
+                                          ctypes.POINTER(_u64),
+                                          ctypes.c_void_p, _u64,
+                                          ctypes.c_void_p, ctypes.c_void_p]),
 }
 
 

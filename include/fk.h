@@ -171,6 +171,27 @@ fk_status fk_batch_stats(const fk_batch* b, fk_stats* out);
 /* The same counters for an engine's last plain call. */
 fk_status fk_engine_stats(const fk_engine* e, fk_stats* out);
 
+/* ---- allocation-free sieve ---------------------------------------------
+ * No counterpart in the reference (its engines allocate through CuPy).
+ * For callers that cannot allocate device memory while they sweep (a fixed
+ * memory budget, an allocator they own, or no implicit synchronisation
+ * allowed): the pre-primality survivors of [lo, hi), as ascending offsets
+ * x - lo, written into the caller's device buffer d_offsets (capacity
+ * entries) with their number in *d_count (a device uint64).  It allocates
+ * nothing: all scratch lives in one fixed device array of about 5.3 MiB
+ * that every GPU loading the library holds until exit.  Limits: at most
+ * 65536 sieve primes and periods * M below 2^55 (else FK_ERR_DOMAIN), and
+ * at most 262144 survivors per call -- more, or more than capacity, makes
+ * *d_count UINT64_MAX.  Asynchronous on `stream` (a cudaStream_t, NULL for
+ * the default stream): synchronise before reading the outputs.  Calls share
+ * the array, so calls that overlap on the GPU race; serialise them.  The
+ * first call on a device (with that device current) looks the array up;
+ * make it before any stream capture.                                      */
+fk_status fk_sieve_noalloc(fk_engine* e, const uint64_t lo[2],
+                           const uint64_t hi[2], uint64_t* d_offsets,
+                           uint64_t capacity, uint64_t* d_count,
+                           void* stream);
+
 /* ---- misc -------------------------------------------------------------- */
 /* Last error message on this thread. */
 const char* fk_last_error(void);

@@ -1,0 +1,85 @@
+"""fk_sieve_noalloc: the allocation-free sieve entry point, on the GPU.
+
+Callers that cannot allocate device memory while they sweep (a fixed
+memory budget, an allocator of their own, no implicit synchronisation
+allowed) call fk_sieve_noalloc with output buffers they own; its scratch
+is a fixed device array inside libfk.  These tests call it through the C
+ABI and require its result to equal the allocating entry point's
+(fk_sieve) exactly -- the streams are integer survivor offsets, so the
+tolerance is zero -- on two calls in a row, so the second call also shows
+that the shared array is reset between calls.
+
+This file is named to be collected last: if it fails, a run that stops
+at the first failure has already run every other test.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CAP = 1 << 18
+
+
+def _bind():
+    import fk_abi
+    lib = fk_abi.load()
+    f = lib.fk_sieve_noalloc
+    f.restype = ctypes.c_int32
+    f.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
+                  ctypes.POINTER(ctypes.c_uint64), ctypes.c_void_p,
+                  ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]
+    return fk_abi, f
+
+
+def _call(f, fk_abi, eng, lo, hi, out, cnt, cap=CAP):
+    import torch
+    st = f(eng.handle, fk_abi.u128(lo), fk_abi.u128(hi), out.data_ptr(),
+           cap, cnt.data_ptr(), None)
+    torch.cuda.synchronize()
+    return st
+
+
+def test_noalloc_equals_fk_sieve_on_two_calls_in_a_row():
+    import torch
+    fk_abi, f = _bind()
+    out = torch.zeros(CAP, dtype=torch.int64, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    cases = [
+        (fk_abi.Engine(fk_abi.EULER, 8, p0=6), 10 ** 5, 10 ** 9),
+        (fk_abi.Engine(fk_abi.AP, 8, q2=4096, p0=6),
+         4 * 10 ** 13 - (4 * 10 ** 13) % 30,
+         4 * 10 ** 13 - (4 * 10 ** 13) % 30 + 3 * 10 ** 6),
+        (fk_abi.Engine(fk_abi.DICKSON, 6, q2=4096, p0=6), 10 ** 6,
+         10 ** 6 + 2 ** 20),
+    ]
+    for eng, lo, hi in cases:
+        want = eng.sieve(lo, hi)
+        assert want.size > 50
+        for _ in range(2):                     # two calls in a row
+            out.fill_(-1)
+            cnt.fill_(-1)
+            assert _call(f, fk_abi, eng, lo, hi, out, cnt) == 0
+            n = int(cnt.item())
+            got = out[:n].cpu().numpy().view(np.uint64)
+            assert n == want.size
+            assert np.array_equal(got, want)
+
+
+def test_noalloc_rejects_what_does_not_fit():
+    import torch
+    fk_abi, f = _bind()
+    out = torch.zeros(16, dtype=torch.int64, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    deep = fk_abi.Engine(fk_abi.DICKSON, 6, q2=1 << 20, p0=6)
+    assert _call(f, fk_abi, deep, 10 ** 6, 10 ** 6 + 1000, out, cnt) == \
+        fk_abi.FK_ERR_DOMAIN                   # 82,000 primes: too many
+    assert b"65536 sieve primes" in fk_abi.load().fk_last_error()
+    eng = fk_abi.Engine(fk_abi.EULER, 8, p0=6)
+    assert _call(f, fk_abi, eng, 10 ** 5, 10 ** 5, out, cnt) == \
+        fk_abi.FK_ERR_DOMAIN                   # empty interval
+    # more survivors than the caller's capacity: count reports UINT64_MAX
+    assert _call(f, fk_abi, eng, 10 ** 5, 10 ** 9, out, cnt, cap=16) == 0
+    assert int(cnt.item()) == -1
