@@ -88,14 +88,18 @@ def dist_env():
 
 
 class Dist:
-    def __init__(self, world, local):
+    """Barrier and max-over-ranks for the timed region (NCCL on GPUs; the
+    CPU tests drive the same code over gloo)."""
+
+    def __init__(self, world, local, backend="nccl"):
         self.world = world
-        self.pg = None
+        self.backend = backend
         if world > 1:
             import torch
             import torch.distributed as td
-            torch.cuda.set_device(local)
-            td.init_process_group("nccl", timeout=datetime.timedelta(
+            if backend == "nccl":
+                torch.cuda.set_device(local)
+            td.init_process_group(backend, timeout=datetime.timedelta(
                 seconds=300))
             self.td, self.torch = td, torch
 
@@ -106,7 +110,8 @@ class Dist:
     def max(self, x):
         if self.world == 1:
             return float(x)
-        t = self.torch.tensor([float(x)], device="cuda", dtype=self.torch.float64)
+        dev = "cuda" if self.backend == "nccl" else "cpu"
+        t = self.torch.tensor([float(x)], device=dev, dtype=self.torch.float64)
         self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
         return float(t.item())
 
@@ -251,6 +256,7 @@ def bench_reference(args):
 def bench_fk(args):
     rank, world, local = dist_env()
     dist = Dist(world, local)
+    import numpy as np
     import torch
     import fk_abi
     import fk_workloads as W
@@ -264,8 +270,13 @@ def bench_fk(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     for _ in range(max(args.warmup, 3)):
-        ref_rows = eng.run(intervals, graph=True)
+        ref_rows = eng.run_arrays(intervals, graph=True)
     torch.cuda.synchronize()
+
+    def same(a, b):
+        return len(a) == len(b) and all(
+            np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
+            for x, y in zip(a, b))
 
     clocks = Clocks(local)
     clocks.start()
@@ -275,14 +286,14 @@ def bench_fk(args):
         torch.cuda.synchronize()
         dist.barrier()
         t0 = time.perf_counter()
-        rows = eng.run(intervals, graph=True)
+        rows = eng.run_arrays(intervals, graph=True)
         t1 = time.perf_counter()
         torch.cuda.synchronize()
         st = eng.stats()
         dev_ms.append(st["total_ms"])
         wall_s.append(t1 - t0)
         stats.append(st)
-        if rows != ref_rows:
+        if not same(rows, ref_rows):
             raise RuntimeError("batched stream changed between steps")
     dist.barrier()
     clk = clocks.stop()
@@ -301,12 +312,12 @@ def bench_fk(args):
     bit_identical = None
     if not args.no_plain:
         pe = PlainEngine(eng.engset)
-        pe.run(intervals[:64])                 # warm
+        pe.run_arrays(intervals[:64])          # warm
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        prow = pe.run(intervals)
+        prow = pe.run_arrays(intervals)
         tp = time.perf_counter() - t0
-        bit_identical = prow == ref_rows
+        bit_identical = same(prow, ref_rows)
         tp = dist.max(tp)
         plain = {"value": cands * world / tp, "unit": UNIT,
                  "ms_per_step": tp * 1e3,
@@ -360,7 +371,6 @@ def bench_fk(args):
     # served workload: continuous batching, p50/p99 latency
     serve = None
     if rank == 0 and world == 1 and not args.no_serve:
-        import numpy as np
         from fk_serve import ServeLoop
         reqs = W.served(count=4000, rate_hz=250.0)
         loop = ServeLoop(eng.engset, slots=2)
@@ -390,7 +400,7 @@ def bench_fk(args):
             "roofline_secondary": secondary,
             "kernel_ms": st_mean,
             "work": {k: st[k] for k in ("candidates", "outputs", "s1_words",
-                                       "s2_tests", "imad_alg",
+                                       "s2_tests", "marks", "imad_alg",
                                        "sprp_values")},
             "e2e": {"value": e2e, "unit": UNIT,
                     "h2d_bytes_per_step": int(st["h2d_bytes"]),

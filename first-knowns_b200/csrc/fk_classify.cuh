@@ -47,42 +47,79 @@ __device__ __forceinline__ void emit_out(const ClassArgs& a, u32 item,
   }
 }
 
-// Euler: f = first x >= 0 with x^2 + x + p failing mr_is_prime, searched
-// up to lim (euler_search.py:258-262, :349-356).
-__device__ u32 euler_first_fail(u128 p, u32 lim, u64* imad) {
+// The values of one candidate's chain (Euler x^2 + x + p for x = t, Dickson
+// (t + 1) * k^2 + 1, AP p + t * d).
+struct Chain {
+  u32 kind;
+  u128 x;   // Euler / AP: p
+  V3 kk;    // Dickson: k^2
+  V3 d;     // AP: difference
+};
+
+__device__ __forceinline__ V3 chain_value(const Chain& c, u32 t) {
+  if (c.kind == KIND_EULER) return v3_from_u128(c.x + (u128)((u64)t * t + t));
+  if (c.kind == KIND_DICKSON) {
+    V3 v = v3_mul_u64(c.kk, (u64)(t + 1));
+    const V3 one = {{1, 0, 0}};
+    return v3_add(v, one);
+  }
+  return v3_add(v3_from_u128(c.x), v3_mul_u64(c.d, (u64)t));
+}
+
+// First t < lim whose value fails sprp_base2 (lim when none does): an
+// upper bound on every engine's depth, because mr_is_prime implies
+// sprp_base2 (huntlib/primes.py:38-46 tests base 2 first).
+__device__ u32 chain_base2(const Chain& c, u32 lim, u64* imad, u64* nval) {
   u32 t = 0;
   while (t < lim) {
-    const V3 v = v3_from_u128(p + (u128)((u64)t * t + t));
-    if (!sprp(v, false, imad)) break;
+    ++*nval;
+    if (!sprp(chain_value(c, t), true, imad)) break;
     ++t;
   }
   return t;
 }
 
-// Dickson: r = largest count with m*k^2 + 1 passing for m = 1..r, capped
-// (ladder_search.py:143-148); base2 selects the launcher's first pass.
-__device__ u32 dickson_run(const V3& kk, u32 cap, bool base2, u64* imad) {
-  u32 r = 0;
-  while (r < cap) {
-    V3 v = v3_mul_u64(kk, (u64)(r + 1));
-    V3 one = {{1, 0, 0}};
-    v = v3_add(v, one);
-    if (!sprp(v, base2, imad)) break;
-    ++r;
+// Every value below d2 passed base 2; the exact mr_is_prime chain ends at
+// the first of them that fails one of the other six bases.
+__device__ u32 chain_exact(const Chain& c, u32 d2, u64* imad, u64* nval) {
+  u32 t = 0;
+  while (t < d2) {
+    ++*nval;
+    if (!sprp_rest(chain_value(c, t), imad)) break;
+    ++t;
   }
-  return r;
+  return t;
 }
 
-// AP chain p + j*d from j = 0, capped (ap_search.py:160-194 when two-pass).
-__device__ u32 ap_run(u128 p, const V3& d, u32 cap, bool base2, u64* imad) {
-  u32 j = 0;
-  V3 v = v3_from_u128(p);
-  while (j < cap) {
-    if (!sprp(v, base2, imad)) break;
-    v = v3_add(v, d);
-    ++j;
+// Depth by the reference's definition for the engine, or -1 when the
+// base-2 bound already proves it below the threshold:
+//   Euler    mr_run_length (euler_search.py:258-262), searched to
+//            max(threshold, cap); hunt keeps f >= threshold, reports
+//            min(f, cap); the dense low pass keeps min(f, cap) >= thr
+//   Dickson  run_length (ladder_search.py:143-148), or the launcher's
+//            two-pass sprp_run (dickson-ladders/launch.py:310-343)
+//   AP       two-pass chain_depth (ap_search.py:160-194)
+__device__ int chain_depth_thr(const Chain& c, u32 mode, u32 thr, u32 cap,
+                               bool two_pass, u64* imad, u64* nval) {
+  if (c.kind == KIND_EULER) {
+    const u32 lim = max(thr, cap);
+    const u32 d2 = chain_base2(c, lim, imad, nval);
+    const bool dense = mode == MODE_DENSE;
+    if ((dense ? min(d2, cap) : d2) < thr) return -1;
+    const u32 f = chain_exact(c, d2, imad, nval);
+    const u32 depth = min(f, cap);
+    return ((dense ? depth : f) >= thr) ? (int)depth : -1;
   }
-  return j;
+  const u32 d2 = chain_base2(c, cap, imad, nval);
+  const u32 pass = (c.kind == KIND_AP) ? 6u : (two_pass ? 5u : 0u);
+  u32 depth;
+  if (d2 < pass) {
+    depth = d2;
+  } else {
+    if (d2 < thr) return -1;
+    depth = chain_exact(c, d2, imad, nval);
+  }
+  return depth >= thr ? (int)depth : -1;
 }
 
 __global__ void __launch_bounds__(kBlock) k_classify(ClassArgs a) {
@@ -100,49 +137,25 @@ __global__ void __launch_bounds__(kBlock) k_classify(ClassArgs a) {
       emit_out(a, item, v << 8);
       continue;
     }
-    const u128 x = (((u128)it.X0_hi << 64) | it.X0_lo) + v;
-    u32 depth = 0;
-    bool keep = false;
-    if (e.kind == KIND_EULER) {
-      const u32 lim = max(it.threshold, it.cap);
-      const u32 f = euler_first_fail(x, lim, &imad);
-      nval += min(f + 1, lim);
-      depth = min(f, it.cap);
-      keep = (it.mode == MODE_DENSE) ? depth >= it.threshold
-                                     : f >= it.threshold;
-    } else if (e.kind == KIND_DICKSON) {
+    Chain c;
+    c.kind = e.kind;
+    c.x = (((u128)it.X0_hi << 64) | it.X0_lo) + v;
+    if (e.kind == KIND_DICKSON) {
       // the line variable is j (k = W*j); a dense item carries k itself
       const u64 W = (it.mode == MODE_DENSE) ? 1ull : e.W;
       bool of = false;
-      const u128 k = x * (u128)W;
-      const V3 kk = v3_mul_128(k, k, &of);
+      const u128 k = c.x * (u128)W;
+      c.kk = v3_mul_128(k, k, &of);
       if (of) {
         atomicOr(&a.ctr->overflow, 8u);
         continue;
       }
-      if (e.two_pass) {
-        depth = dickson_run(kk, it.cap, true, &imad);
-        nval += min(depth + 1, it.cap);
-        if (depth >= 5) {
-          depth = dickson_run(kk, it.cap, false, &imad);
-          nval += min(depth + 1, it.cap);
-        }
-      } else {
-        depth = dickson_run(kk, it.cap, false, &imad);
-        nval += min(depth + 1, it.cap);
-      }
-      keep = depth >= it.threshold;
-    } else {
-      const V3 d = {{e.d_lo, e.d_hi, 0}};
-      depth = ap_run(x, d, it.cap, true, &imad);
-      nval += min(depth + 1, it.cap);
-      if (depth >= 6) {
-        depth = ap_run(x, d, it.cap, false, &imad);
-        nval += min(depth + 1, it.cap);
-      }
-      keep = depth >= it.threshold;
+    } else if (e.kind == KIND_AP) {
+      c.d = V3{{e.d_lo, e.d_hi, 0}};
     }
-    if (keep) emit_out(a, item, (v << 8) | (u64)min(depth, 255u));
+    const int depth = chain_depth_thr(c, it.mode, it.threshold, it.cap,
+                                      e.two_pass != 0, &imad, &nval);
+    if (depth >= 0) emit_out(a, item, (v << 8) | (u64)min((u32)depth, 255u));
   }
   // one atomic per warp for the work counters
   u64 s1 = imad, s2 = nval;

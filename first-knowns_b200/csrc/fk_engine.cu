@@ -123,6 +123,7 @@ struct fk_engine {
   double survival = 1.0;      // expected survival through every sieve prime
   bool use_mark = false;      // long lanes go to the marking sieve
   bool force_mark = false;    // every item goes to the marking sieve
+  double c_round = 0, c_mark_bit = 0, c_mark_seg = 0, c_mark_lane = 0;
   double test_cost = 0, mark_cost = 0;
   DevEngine dev{};
   std::vector<void*> allocs;
@@ -372,27 +373,39 @@ static fk_status build_engine(fk_engine* e) {
     glist.insert(glist.end(), g.begin(), g.end());
   }
   if (glist.size() >= (1u << 24)) return set_err(FK_ERR_DOMAIN, "glist too large");
-  // cost model (instructions per post-wheel candidate): per-candidate
-  // rounds test every survivor against every remaining prime; marking
-  // pays one byte store per hit plus a per-segment setup per prime
+  // cost model, in instructions per post-wheel candidate (one lane-period):
+  // both kernels run the same pattern stage; the rounds then test each
+  // pattern survivor against every remaining prime until one kills it,
+  // the marking sieve pays one byte store per hit plus, per lane, a
+  // per-segment setup for every marked prime and a per-task shift table
   {
-    double test_cost = 0, mark_cost = 0, surv = 1.0;
+    double s1 = 1.0;
+    for (u32 i = 0; i < (u32)kNS && i < NP; ++i)
+      s1 *= 1.0 - (double)e->forb[i].size() / e->sieve[i];
+    double tests = 0, surv = 1.0, mark_bit = 0, seg = 0, tail = 0;
+    double surv_m = 1.0;
     for (u32 i = kNS; i < NP; ++i) {
       const double kill = (double)e->forb[i].size() / e->sieve[i];
-      test_cost += 22.0 * surv;
-      if (i < NPm) {
-        mark_cost += 4.0 * kill + (12.0 + 4.0 * e->forb[i].size()) / kSeg;
-      } else {
-        mark_cost += 22.0 * surv;
-      }
+      tests += surv;
       surv *= 1.0 - kill;
+      if (i < NPm) {
+        mark_bit += kill;
+        seg += 12.0 + 4.0 * e->forb[i].size();
+        surv_m *= 1.0 - kill;
+      } else {
+        tail += surv_m;
+        surv_m *= 1.0 - kill;
+      }
     }
-    e->use_mark = NPm > (u32)kNS && mark_cost < test_cost;
+    e->c_round = 2.5 + 22.0 * s1 * tests;
+    e->c_mark_bit = 2.5 + 2.0 + 4.0 * mark_bit + 22.0 * s1 * tail;
+    e->c_mark_seg = seg + 2048.0;
+    e->c_mark_lane = 15.0 * (NPm > (u32)kNS ? NPm - kNS : 0);
+    e->use_mark = NPm > (u32)kNS;
     if (p.sieve == 1) e->use_mark = false;
-    if (p.sieve == 2) e->use_mark = NPm > (u32)kNS;
     e->force_mark = p.sieve == 2 && e->use_mark;
-    e->test_cost = test_cost;
-    e->mark_cost = mark_cost;
+    e->test_cost = e->c_round;
+    e->mark_cost = e->c_mark_bit;
   }
   // ---- upload -------------------------------------------------------------
   DevEngine& d = e->dev;
@@ -596,8 +609,6 @@ static int fam_of(u32 P0, bool mark) {
   return (P0 == 3 ? 0 : P0 == 6 ? 1 : P0 == 9 ? 2 : 3) + (mark ? 4 : 0);
 }
 
-// Periods per lane below which an item stays on the per-candidate kernel.
-static const u64 kMarkMinPeriods = 4ull * kSeg;
 
 // Largest value a chain can produce must fit three limbs.
 static bool chain_fits(const fk_engine* e, u128 x_hi, u32 cap, bool dense) {
@@ -671,7 +682,16 @@ static fk_status expand(fk_batch* b, const fk_item* items, u64 nitems) {
       di.lo_off = (s0 == 0) ? (u64)(lo - X0) : 0;
       const bool last = s0 + U >= periods;
       di.hi_last = last ? (u64)(hi - (base + (u128)(U - 1) * M)) : M;
-      const bool mark = e->use_mark && (U >= kMarkMinPeriods || e->force_mark);
+      bool mark = false;
+      if (e->use_mark) {
+        const double Ud = (double)U;
+        const double rounds = Ud * e->c_round;
+        const double tasks = std::ceil(Ud / ((double)kSeg * kSegPerTask));
+        const double segs = std::ceil(Ud / kSeg);
+        const double marking = tasks * e->c_mark_lane + segs * e->c_mark_seg +
+                               Ud * e->c_mark_bit;
+        mark = e->force_mark || marking < rounds;
+      }
       di.marked = mark ? 1 : 0;
       if (mark) {
         di.nchunk_u = (U + (u64)kSeg * kSegPerTask - 1) / ((u64)kSeg * kSegPerTask);
@@ -1276,31 +1296,27 @@ __global__ void k_sprp_vals(const u64* v, u64 n, int base2, uint8_t* out) {
   }
 }
 
+// Exact chain depth of explicit chain starts (no threshold): Euler
+// mr_run_length(p, cap), Dickson run_length(k, cap) (or the two-pass
+// sprp_run), AP two-pass chain_depth(p, cap).
 __global__ void k_depth_vals(DevEngine e, const u64* x, u64 n, u32 cap,
                              uint8_t* out) {
   for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (u64)gridDim.x * blockDim.x) {
     const u128 v = ((u128)x[2 * i + 1] << 64) | x[2 * i];
-    u32 depth = 0;
-    u64 im = 0;
-    if (e.kind == KIND_EULER) {
-      depth = euler_first_fail(v, cap, &im);
-    } else if (e.kind == KIND_DICKSON) {
-      bool of = false;
-      const V3 kk = v3_mul_128(v, v, &of);
-      if (e.two_pass) {
-        depth = dickson_run(kk, cap, true, &im);
-        if (depth >= 5) depth = dickson_run(kk, cap, false, &im);
-      } else {
-        depth = dickson_run(kk, cap, false, &im);
-      }
-      if (of) depth = 255;
-    } else {
-      const V3 d = {{e.d_lo, e.d_hi, 0}};
-      depth = ap_run(v, d, cap, true, &im);
-      if (depth >= 6) depth = ap_run(v, d, cap, false, &im);
-    }
-    out[i] = (uint8_t)min(depth, 255u);
+    u64 im = 0, nv = 0;
+    Chain c;
+    c.kind = e.kind;
+    c.x = v;
+    bool of = false;
+    if (e.kind == KIND_DICKSON) c.kk = v3_mul_128(v, v, &of);
+    if (e.kind == KIND_AP) c.d = V3{{e.d_lo, e.d_hi, 0}};
+    int depth;
+    if (e.kind == KIND_EULER)
+      depth = chain_depth_thr(c, MODE_DENSE, 0, cap, false, &im, &nv);
+    else
+      depth = chain_depth_thr(c, MODE_HUNT, 0, cap, e.two_pass != 0, &im, &nv);
+    out[i] = of ? 255 : (uint8_t)min((u32)depth, 255u);
   }
 }
 

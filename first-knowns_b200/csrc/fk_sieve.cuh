@@ -173,6 +173,45 @@ __device__ void drain(SieveSmem& S, u32 n, const DevEngine& e,
   const u64 M = e.M;
   for (u32 r = 0; r < e.nrounds && n > 0; ++r) {
     const u32 i0 = __ldg(e.rounds + r), i1 = __ldg(e.rounds + r + 1);
+    if (n < (u32)kWarpMode) {
+      // Sparse queue: one warp per candidate over every remaining prime,
+      // the lanes splitting the primes 32 at a time and voting after each
+      // group (the reference's warp-per-candidate deep rounds,
+      // dickson-ladders/ladder_gpu.py:378-407), so a lone deep survivor
+      // no longer runs thousands of primes on one lane of an idle warp.
+      const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+      for (u32 idx = wid; idx < n; idx += kBlock / 32) {
+        const u32 code = qin[idx];
+        const u32 t = code >> 22;
+        const u64 u = 64ull * (S.chain_w0[t] + ((code >> 6) & 0xFFFFu)) +
+                      (code & 63u);
+        const u64 v = u * M + S.chain_R[t];
+        bool dead = false;
+        for (u32 b = i0; b < e.NP && !dead; b += 32) {
+          const u32 i = b + lane;
+          bool kill = false;
+          if (i < e.NP) {
+            const PrimeRec pr = e.recs[i];
+            u32 rr = fk_bmod(v, pr.q, pr.magic) + __ldg(xq + i);
+            rr = min(rr, rr - pr.q);
+            kill = kill_test<KIND>(pr, rr, e.lists, S.sbits, e.xxmax, e.n);
+            ++ntest;
+          }
+          dead = __any_sync(0xffffffffu, kill);
+        }
+        if (!dead && lane == 0) {
+          const unsigned long long p = atomicAdd(&a.ctr->ncand, 1ull);
+          if (p < a.cand_cap) {
+            a.cand_key[p] = v;
+            a.cand_item[p] = gitem;
+          } else {
+            atomicOr(&a.ctr->overflow, 1u);
+          }
+        }
+      }
+      __syncthreads();
+      return;
+    }
     u32 mask = 0;
     int k = 0;
     for (u32 idx = threadIdx.x; idx < n; idx += kBlock, ++k) {

@@ -176,116 +176,170 @@ __device__ __forceinline__ u32 small_mod(const u64* m, u32 s, u32 c) {
   return (u32)r;
 }
 
-// huntlib/primes.py:23-80 for an L-limb m whose top limb is nonzero.
-// nbases = 7 gives mr_is_prime, nbases = 1 gives sprp_base2.
+// Trial division of huntlib/primes.py:31-33 by the primes 2..37:
+// returns 0 (composite: divisible by a small prime it is not), 1 (m is one
+// of those primes, prime), or 2 (no small factor: go on).  Uses two
+// composite moduli, 223092870 = 2*3*5*7*11*13*17*19*23 and 33263 = 29*31*37.
 template <int L>
-__device__ bool sprp_L(const u64* m, int nbases, u64* imad) {
-  if (L == 1 && m[0] < 2) return false;
-  // trial division by 2..37 via two composite moduli
-  // 223092870 = 2*3*5*7*11*13*17*19*23 ; 33263 = 29*31*37
-  const u32 r1 = small_mod<L>(m, 223092870u, (u32)(18446744073709551615ull % 223092870ull + 1) % 223092870u);
-  const u32 r2 = small_mod<L>(m, 33263u, (u32)(18446744073709551615ull % 33263ull + 1) % 33263u);
+__device__ __forceinline__ int trial_small(const u64* m) {
+  if (L == 1 && m[0] < 2) return 0;
+  const u32 r1 = small_mod<L>(
+      m, 223092870u, (u32)((18446744073709551615ull % 223092870ull + 1) % 223092870ull));
+  const u32 r2 = small_mod<L>(
+      m, 33263u, (u32)((18446744073709551615ull % 33263ull + 1) % 33263ull));
   const u32 sp1[9] = {2, 3, 5, 7, 11, 13, 17, 19, 23};
   const u32 sp2[3] = {29, 31, 37};
 #pragma unroll
   for (int i = 0; i < 9; ++i)
-    if (r1 % sp1[i] == 0) return L == 1 && m[0] == sp1[i];
+    if (r1 % sp1[i] == 0) return (L == 1 && m[0] == sp1[i]) ? 1 : 0;
 #pragma unroll
   for (int i = 0; i < 3; ++i)
-    if (r2 % sp2[i] == 0) return L == 1 && m[0] == sp2[i];
+    if (r2 % sp2[i] == 0) return (L == 1 && m[0] == sp2[i]) ? 1 : 0;
+  return 2;
+}
 
-  // m odd and > 37 here.  Montgomery constants.
-  u64 minv = m[0];  // inverse mod 2^3
+// Montgomery context of an odd m > 37 with no small factor.
+template <int L>
+struct Ctx {
+  u64 m[L], one[L], mone[L], d[L];
+  u64 minv;
+  int bl, s, dtop;
+};
+
+template <int L>
+__device__ __forceinline__ void ctx_init(Ctx<L>& c, const u64* m) {
+#pragma unroll
+  for (int i = 0; i < L; ++i) c.m[i] = m[i];
+  u64 minv = m[0];  // m * m == 1 mod 8: correct to 3 bits
 #pragma unroll
   for (int i = 0; i < 5; ++i) minv *= 2 - m[0] * minv;
-  minv = (u64)0 - minv;  // -m^-1 mod 2^64
-
-  const int bl = bitlen_top<L>(m);
-  u64 one[L], r2m[L];
+  c.minv = (u64)0 - minv;  // -m^-1 mod 2^64
+  c.bl = bitlen_top<L>(m);
 #pragma unroll
-  for (int i = 0; i < L; ++i) one[i] = 0;
-  one[(bl - 1) >> 6] = 1ull << ((bl - 1) & 63);  // 2^(bl-1) < m
-  for (int i = 0; i < 64 * L - bl + 1; ++i) mod_double<L>(one, m);  // R mod m
+  for (int i = 0; i < L; ++i) c.one[i] = 0;
+  c.one[(c.bl - 1) >> 6] = 1ull << ((c.bl - 1) & 63);  // 2^(bl-1) < m
+  for (int i = 0; i < 64 * L - c.bl + 1; ++i) mod_double<L>(c.one, m);
+  u64 br = 0;
 #pragma unroll
-  for (int i = 0; i < L; ++i) r2m[i] = one[i];
-  for (int i = 0; i < 64 * L; ++i) mod_double<L>(r2m, m);  // R^2 mod m
-  u64 mone[L];  // m - one  == -1 in Montgomery form
-  {
-    u64 br = 0;
-#pragma unroll
-    for (int i = 0; i < L; ++i) {
-      u64 x = m[i] - one[i];
-      u64 b1 = m[i] < one[i];
-      u64 x2 = x - br;
-      u64 b2 = x < br;
-      mone[i] = x2;
-      br = b1 | b2;
-    }
+  for (int i = 0; i < L; ++i) {  // m - (R mod m): -1 in Montgomery form
+    const u64 x = m[i] - c.one[i];
+    const u64 b1 = m[i] < c.one[i];
+    const u64 x2 = x - br;
+    const u64 b2 = x < br;
+    c.mone[i] = x2;
+    br = b1 | b2;
   }
-  // d = (m - 1) >> s
-  u64 d[L];
 #pragma unroll
-  for (int i = 0; i < L; ++i) d[i] = m[i];
-  d[0] -= 1;  // m odd: no borrow
-  int s = 0;
-  {
-    int lz = 0;
-    while (d[lz] == 0) ++lz;  // d != 0 since m > 37
-    s = 64 * lz + __ffsll((long long)d[lz]) - 1;
-    // shift right by s
-    const int ws = s >> 6, bs = s & 63;
+  for (int i = 0; i < L; ++i) c.d[i] = m[i];
+  c.d[0] -= 1;  // m odd
+  int lz = 0;
+  while (c.d[lz] == 0) ++lz;
+  c.s = 64 * lz + __ffsll((long long)c.d[lz]) - 1;
+  const int ws = c.s >> 6, bs = c.s & 63;
 #pragma unroll
-    for (int i = 0; i < L; ++i) {
-      u64 lo = (i + ws < L) ? d[i + ws] : 0;
-      u64 hi = (i + ws + 1 < L) ? d[i + ws + 1] : 0;
-      d[i] = bs ? ((lo >> bs) | (hi << (64 - bs))) : lo;
-    }
+  for (int i = 0; i < L; ++i) {
+    const u64 lo = (i + ws < L) ? c.d[i + ws] : 0;
+    const u64 hi = (i + ws + 1 < L) ? c.d[i + ws + 1] : 0;
+    c.d[i] = bs ? ((lo >> bs) | (hi << (64 - bs))) : lo;
   }
-  int dtop = 0;  // index of the top set bit of d
+  c.dtop = 0;
 #pragma unroll
   for (int i = L - 1; i >= 0; --i)
-    if (d[i] && dtop == 0) dtop = 64 * i + 63 - __clzll(d[i]);
+    if (c.d[i] && c.dtop == 0) c.dtop = 64 * i + 63 - __clzll(c.d[i]);
+}
 
-  // algorithmic work of one strong test (32-bit CIOS): (bits - 1) squarings
-  // of 2l^2 + l word products, each a lo and a hi multiply-add
-  const u64 l32 = (u64)((bl + 31) >> 5);
-  const u64 per_base = (u64)(bl - 1) * (4 * l32 * l32 + 2 * l32);
-  for (int bi = 0; bi < nbases; ++bi) {
+// Algorithmic 32-bit multiply-adds of one strong test (CIOS on 32-bit
+// limbs): (bits - 1) squarings of 2l^2 + l word products, lo and hi each.
+template <int L>
+__device__ __forceinline__ u64 imad_per_base(const Ctx<L>& c) {
+  const u64 l32 = (u64)((c.bl + 31) >> 5);
+  return (u64)(c.bl - 1) * (4 * l32 * l32 + 2 * l32);
+}
+
+// The strong-test tail: x = a^d already in Montgomery form.
+template <int L>
+__device__ __forceinline__ bool strong_tail(const Ctx<L>& c, u64* x) {
+  if (limbs_eq<L>(x, c.one) || limbs_eq<L>(x, c.mone)) return true;
+  for (int r = 1; r < c.s; ++r) {
+    mont_mul<L>(x, x, x, c.m, c.minv);
+    if (limbs_eq<L>(x, c.mone)) return true;
+  }
+  return false;
+}
+
+// Strong test to base 2: left-to-right over d by squaring and modular
+// doubling, so no R^2 table is needed.
+template <int L>
+__device__ __forceinline__ bool base2(const Ctx<L>& c, u64* imad) {
+  *imad += imad_per_base<L>(c);
+  u64 x[L];
+#pragma unroll
+  for (int i = 0; i < L; ++i) x[i] = c.one[i];
+  for (int b = c.dtop; b >= 0; --b) {
+    mont_mul<L>(x, x, x, c.m, c.minv);
+    if ((c.d[b >> 6] >> (b & 63)) & 1) mod_double<L>(x, c.m);
+  }
+  return strong_tail<L>(c, x);
+}
+
+// Strong tests to the six other bases of huntlib's set, with a %= m and a
+// zero base skipped (huntlib/primes.py:38-46).
+template <int L>
+__device__ bool bases_rest(const Ctx<L>& c, u64* imad) {
+  u64 r2m[L];
+#pragma unroll
+  for (int i = 0; i < L; ++i) r2m[i] = c.one[i];
+  for (int i = 0; i < 64 * L; ++i) mod_double<L>(r2m, c.m);  // R^2 mod m
+  for (int bi = 1; bi < 7; ++bi) {
     u64 a = kMrBases[bi];
-    if (L == 1 && m[0] <= a) {
-      a %= m[0];
+    if (L == 1 && c.m[0] <= a) {
+      a %= c.m[0];
       if (a == 0) continue;
     }
+    *imad += imad_per_base<L>(c);
     u64 av[L], at[L], x[L];
 #pragma unroll
     for (int i = 0; i < L; ++i) av[i] = 0;
     av[0] = a;
-    *imad += per_base;
-    mont_mul<L>(at, av, r2m, m, minv);  // a * R mod m
+    mont_mul<L>(at, av, r2m, c.m, c.minv);  // a * R mod m
 #pragma unroll
     for (int i = 0; i < L; ++i) x[i] = at[i];
-    for (int b = dtop - 1; b >= 0; --b) {
-      mont_mul<L>(x, x, x, m, minv);
-      if ((d[b >> 6] >> (b & 63)) & 1) mont_mul<L>(x, x, at, m, minv);
+    for (int b = c.dtop - 1; b >= 0; --b) {
+      mont_mul<L>(x, x, x, c.m, c.minv);
+      if ((c.d[b >> 6] >> (b & 63)) & 1) mont_mul<L>(x, x, at, c.m, c.minv);
     }
-    if (limbs_eq<L>(x, one) || limbs_eq<L>(x, mone)) continue;
-    bool ok = false;
-    for (int r = 1; r < s; ++r) {
-      mont_mul<L>(x, x, x, m, minv);
-      if (limbs_eq<L>(x, mone)) { ok = true; break; }
-    }
-    if (!ok) return false;
+    if (!strong_tail<L>(c, x)) return false;
   }
   return true;
 }
 
-// Dispatch on the limb count of v.  base2_only selects sprp_base2.  *imad
-// accumulates the algorithmic multiply-add count of the bases run.
-__device__ __noinline__ bool sprp(const V3& v, bool base2_only, u64* imad) {
-  const int nb = base2_only ? 1 : 7;
-  if (v.w[2]) return sprp_L<3>(v.w, nb, imad);
-  if (v.w[1]) return sprp_L<2>(v.w, nb, imad);
-  return sprp_L<1>(v.w, nb, imad);
+// which = 0: mr_is_prime, 1: sprp_base2, 2: the six bases after 2 only
+// (callers that already know m passes base 2).
+template <int L>
+__device__ bool sprp_L(const u64* m, int which, u64* imad) {
+  const int t = trial_small<L>(m);
+  if (t != 2) return t == 1;
+  Ctx<L> c;
+  ctx_init<L>(c, m);
+  if (which != 2 && !base2<L>(c, imad)) return false;
+  if (which == 1) return true;
+  return bases_rest<L>(c, imad);
+}
+
+__device__ __noinline__ bool sprp_which(const V3& v, int which, u64* imad) {
+  if (v.w[2]) return sprp_L<3>(v.w, which, imad);
+  if (v.w[1]) return sprp_L<2>(v.w, which, imad);
+  return sprp_L<1>(v.w, which, imad);
+}
+
+// mr_is_prime (base2_only = false) or sprp_base2 (true).
+__device__ __forceinline__ bool sprp(const V3& v, bool base2_only, u64* imad) {
+  return sprp_which(v, base2_only ? 1 : 0, imad);
+}
+
+// The six bases after 2 (v already passed base 2 and trial division).
+__device__ __forceinline__ bool sprp_rest(const V3& v, u64* imad) {
+  return sprp_which(v, 2, imad);
 }
 
 }  // namespace fk

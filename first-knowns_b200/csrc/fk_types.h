@@ -25,6 +25,7 @@ constexpr int kQcap = 4096;       // per-CTA candidate queue (entries)
 constexpr int kNS = 32;           // pattern primes per chain
 constexpr int kMaxRounds = 64;
 constexpr int kSortSmem = 4096;   // entries a CTA sorts in shared memory
+constexpr int kWarpMode = 512;    // queue below which rounds go warp-wide
 constexpr int kSeg = 32768;       // marking: periods per shared segment
 constexpr int kSegPerTask = 8;    // marking: segments per task
 

@@ -83,6 +83,14 @@ class BatchEngine:
             self._nengines = n
         return self._batch
 
+    def run_arrays(self, intervals, graph=True):
+        """Per interval, (offsets, depths) as numpy arrays, ascending, in
+        the engine's device line variable: x = lo + offset for Euler and
+        AP, k = W * (ceil(lo / W) + offset) for Dickson.  No per-hit
+        Python objects: the form to use at high hit rates."""
+        specs = item_specs(self.engset, intervals)
+        return self._ensure().run(specs, graph=graph)
+
     def run(self, intervals, graph=True):
         """[(x, depth)] per interval, ascending, depth >= threshold."""
         specs = item_specs(self.engset, intervals)
@@ -99,6 +107,10 @@ class BatchEngine:
         specs = item_specs(self.engset, intervals)
         self._pending = list(intervals)
         self._ensure().submit(specs, graph=graph)
+
+    def wait_arrays(self):
+        """The submitted run's per-interval (offsets, depths) arrays."""
+        return self._batch.wait()
 
     def wait(self):
         rows = self._batch.wait()
@@ -123,6 +135,15 @@ class PlainEngine:
 
     def __init__(self, engset=None):
         self.engset = engset or EngineSet()
+
+    def run_arrays(self, intervals):
+        """Per interval (offsets, depths) as BatchEngine.run_arrays."""
+        out = []
+        for iv in intervals:
+            e = self.engset.get(engine_key(iv))
+            lo, hi = line_range(iv, e.W if iv.kind == DICKSON else 1)
+            out.append(e.hunt(lo, hi, iv.threshold, iv.cap))
+        return out
 
     def run(self, intervals):
         out = []

@@ -71,7 +71,7 @@ class ServeLoop:
             for si in list(inflight):
                 if self.slots[si]._batch.ready():
                     ids = inflight.pop(si)
-                    rows = self.slots[si].wait()
+                    rows = self.slots[si].wait_arrays()
                     done = time.perf_counter() - t0
                     st = self.slots[si].stats()
                     busy_s += st["total_ms"] * 1e-3

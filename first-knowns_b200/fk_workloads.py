@@ -114,6 +114,13 @@ def served(count=2000, rate_hz=200.0, seed=SEED + 1):
     return out
 
 
+def shard(intervals, rank, world):
+    """The intervals rank `rank` of `world` sweeps: a round-robin split of
+    the list, disjoint across ranks and covering it (no interval is cut,
+    so no survivor is shared and no collective is needed)."""
+    return [iv for i, iv in enumerate(intervals) if i % world == rank]
+
+
 def total_length(intervals):
     return sum(iv.length for iv in intervals)
 

@@ -23,7 +23,10 @@ EULER, DICKSON, AP = 0, 1, 2
 
 @functools.lru_cache(maxsize=16)
 def _euler(n):
-    return euler.CpuEngine(n)
+    # the survivor set does not depend on the wheel (euler_search.py:1-20);
+    # the 23# table keeps small n affordable (29# has 3.5e7 offsets at n=4)
+    wheel = euler.WHEEL_PRIMES if n <= 8 else euler.WHEEL_PRIMES_29
+    return euler.CpuEngine(n, wheel)
 
 
 @functools.lru_cache(maxsize=16)

@@ -1,0 +1,111 @@
+"""The batched and served engines: identical to the plain engine.
+
+One persistent launch over many intervals of mixed engine type must give,
+for every interval, exactly the stream the plain per-interval call gives,
+whether replayed from a captured CUDA graph or launched eagerly, and
+whether the interval runs alone or in a mix; the serving loop must return
+the same results for requests that overlap on the device.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _clipped(count, seed, clip=1 << 26):
+    import fk_workloads as W
+    out = []
+    for iv in W.mixed_batch(count, seed):
+        hi = min(iv.hi, iv.lo + clip)
+        if iv.kind == W.AP:
+            hi = iv.lo + max(30, (hi - iv.lo) // 30 * 30)
+        out.append(W.Interval(iv.kind, iv.n, iv.lo, hi, iv.threshold, iv.cap))
+    return out
+
+
+def _same(a, b):
+    return len(a) == len(b) and all(
+        np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
+        for x, y in zip(a, b))
+
+
+def test_batch_equals_plain_graph_and_eager():
+    from fk_batch import BatchEngine, PlainEngine
+    ivs = _clipped(300, 77)
+    be = BatchEngine(ivs)
+    g1 = be.run_arrays(ivs, graph=True)
+    g2 = be.run_arrays(ivs, graph=True)          # graph replay
+    e1 = be.run_arrays(ivs, graph=False)
+    p = PlainEngine(be.engset).run_arrays(ivs)
+    assert _same(g1, g2) and _same(g1, e1) and _same(g1, p)
+    assert sum(x[0].size for x in g1) > 100
+
+
+def test_alone_equals_in_the_mix():
+    from fk_batch import BatchEngine
+    ivs = _clipped(120, 78)
+    be = BatchEngine(ivs)
+    mix = be.run(ivs)
+    for i in (0, 7, 33, 119):
+        assert be.run([ivs[i]])[0] == mix[i]
+
+
+def test_batch_equals_oracle_on_a_sample():
+    from fk_batch import BatchEngine
+    from oracle import sweep
+    ivs = _clipped(24, 79, clip=1 << 21)
+    got = BatchEngine(ivs).run(ivs)
+    for iv, g in zip(ivs, got):
+        assert g == sweep.hunt_interval(iv.kind, iv.n, iv.lo, iv.hi,
+                                        iv.threshold, iv.cap, iv.q2, iv.d)
+
+
+def test_full_length_intervals_through_the_marking_sieve():
+    """Unclipped long intervals (the marking kernel's territory) agree
+    between the batch and the plain engine, and the batch stats show the
+    marking sieve ran."""
+    import fk_workloads as W
+    from fk_batch import BatchEngine, PlainEngine
+    ivs = [iv for iv in W.mixed_batch(200, 80) if iv.length > 2 ** 33][:6]
+    be = BatchEngine(ivs)
+    got = be.run_arrays(ivs)
+    assert be.stats()["marks"] > 0
+    assert _same(got, PlainEngine(be.engset).run_arrays(ivs))
+
+
+def test_serving_loop_matches_plain_results():
+    import fk_workloads as W
+    from fk_batch import PlainEngine
+    from fk_serve import ServeLoop
+    reqs = []
+    for t, iv in W.served(count=150, rate_hz=400.0):
+        hi = min(iv.hi, iv.lo + (1 << 24))
+        if iv.kind == W.AP:
+            hi = iv.lo + max(30, (hi - iv.lo) // 30 * 30)
+        reqs.append((t, W.Interval(iv.kind, iv.n, iv.lo, hi, iv.threshold,
+                                   iv.cap)))
+    loop = ServeLoop(slots=2, max_items=32)
+    res, lat, st = loop.run(reqs)
+    assert st["requests"] == len(reqs) and st["batches"] > 1
+    assert np.all(lat >= 0)
+    plain = PlainEngine(loop.engset).run_arrays([iv for _, iv in reqs])
+    assert _same(res, plain)
+
+
+def test_submit_ready_wait():
+    import fk_abi
+    from fk_batch import BatchEngine
+    ivs = _clipped(40, 81)
+    be = BatchEngine(ivs)
+    want = be.run_arrays(ivs, graph=False)
+    be.submit(ivs)
+    import time
+    t0 = time.time()
+    while not be._batch.ready():
+        assert time.time() - t0 < 60
+        time.sleep(0.001)
+    assert _same(be.wait_arrays(), want)
+    st = be.stats()
+    assert st["launches"] >= 5 and st["total_ms"] > 0
+    assert fk_abi.peak("imad") > 1e12
