@@ -122,40 +122,154 @@ __device__ int chain_depth_thr(const Chain& c, u32 mode, u32 thr, u32 cap,
   return depth >= thr ? (int)depth : -1;
 }
 
+// The SPRP stage as a step interpreter.  Each lane holds the state of one
+// candidate's chain and performs exactly ONE strong test per step -- one
+// value, one base -- then advances its own state machine:
+//   phase 0  base-2 chain: test value t to base 2; pass -> t + 1 (until the
+//            limit), fail -> d2 = t, the base-2 depth, an upper bound on
+//            every engine's depth (mr_is_prime implies sprp_base2)
+//   decide   by the engine's rules (chain_depth_thr): drop the candidate
+//            when d2 already proves it below the threshold, report d2 for
+//            the two-pass engines below their exact-from depth, else
+//   phase 1  the exact chain: values t < d2 tested to the six other bases,
+//            one base per step; the first failure ends the chain
+// A lane whose candidate is finished takes the next one at once from a
+// chunk its warp fetched, so a warp never waits for its longest chain, and
+// lanes of one warp run the same loop shape on same-sized values.
+struct LaneState {
+  Chain c;
+  u64 v;
+  u32 item, mode, thr, cap;
+  u32 phase, t, bi, lim, d2, pass;
+};
+
+__device__ __forceinline__ bool lane_init(LaneState& s, const ClassArgs& a,
+                                          u64 i) {
+  s.item = a.cand_item[i];
+  const DevItem it = a.items[s.item];
+  const DevEngine& e = a.engines[it.engine];
+  s.v = a.cand_key[i];
+  if (it.mode == MODE_SIEVE) {
+    emit_out(a, s.item, s.v << 8);
+    return false;
+  }
+  s.mode = it.mode;
+  s.thr = it.threshold;
+  s.cap = it.cap;
+  s.c.kind = e.kind;
+  s.c.x = (((u128)it.X0_hi << 64) | it.X0_lo) + s.v;
+  if (e.kind == KIND_DICKSON) {
+    const u64 W = (it.mode == MODE_DENSE) ? 1ull : e.W;
+    bool of = false;
+    const u128 k = s.c.x * (u128)W;
+    s.c.kk = v3_mul_128(k, k, &of);
+    if (of) {
+      atomicOr(&a.ctr->overflow, 8u);
+      return false;
+    }
+  } else if (e.kind == KIND_AP) {
+    s.c.d = V3{{e.d_lo, e.d_hi, 0}};
+  }
+  s.pass = (e.kind == KIND_AP) ? 6u
+           : (e.kind == KIND_DICKSON ? (e.two_pass ? 5u : 0u) : 0u);
+  s.lim = (e.kind == KIND_EULER) ? max(s.thr, s.cap) : s.cap;
+  s.phase = 0;
+  s.t = 0;
+  s.bi = 0;
+  return true;
+}
+
+// Finish with the exact depth: emit when it reaches the threshold.
+__device__ __forceinline__ void lane_final(const LaneState& s,
+                                           const ClassArgs& a, u32 exact) {
+  if (s.c.kind == KIND_EULER) {
+    const u32 depth = min(exact, s.cap);
+    const u32 test = (s.mode == MODE_DENSE) ? depth : exact;
+    if (test >= s.thr) emit_out(a, s.item, (s.v << 8) | (u64)min(depth, 255u));
+  } else if (exact >= s.thr) {
+    emit_out(a, s.item, (s.v << 8) | (u64)min(exact, 255u));
+  }
+}
+
+// After the base-2 chain: returns true when the exact phase must run.
+__device__ __forceinline__ bool lane_decide(LaneState& s, const ClassArgs& a) {
+  const u32 d2 = s.d2;
+  if (s.c.kind == KIND_EULER) {
+    const u32 bound = (s.mode == MODE_DENSE) ? min(d2, s.cap) : d2;
+    if (bound < s.thr) return false;
+  } else {
+    if (d2 < s.pass) {
+      if (d2 >= s.thr) emit_out(a, s.item, (s.v << 8) | (u64)min(d2, 255u));
+      return false;
+    }
+    if (d2 < s.thr) return false;
+  }
+  if (d2 == 0) {
+    lane_final(s, a, 0);
+    return false;
+  }
+  s.phase = 1;
+  s.t = 0;
+  s.bi = 1;
+  return true;
+}
+
 __global__ void __launch_bounds__(kBlock) k_classify(ClassArgs a) {
   u64 n = a.ctr->ncand;
   if (n > a.cand_cap) n = a.cand_cap;
-  const u64 stride = (u64)gridDim.x * blockDim.x;
+  const u32 lane = threadIdx.x & 31;
+  const u32 lt = (1u << lane) - 1u;
+  u64 chunk_pos = 0, chunk_end = 0;  // warp-uniform
+  bool active = false, drained = false;
+  LaneState st;
   u64 imad = 0, nval = 0;
-  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += stride) {
-    const u32 item = a.cand_item[i];
-    const DevItem it = a.items[item];
-    const DevEngine& e = a.engines[it.engine];
-    const u64 v = a.cand_key[i];
-    if (it.mode == MODE_SIEVE) {
-      emit_out(a, item, v << 8);
-      continue;
-    }
-    Chain c;
-    c.kind = e.kind;
-    c.x = (((u128)it.X0_hi << 64) | it.X0_lo) + v;
-    if (e.kind == KIND_DICKSON) {
-      // the line variable is j (k = W*j); a dense item carries k itself
-      const u64 W = (it.mode == MODE_DENSE) ? 1ull : e.W;
-      bool of = false;
-      const u128 k = c.x * (u128)W;
-      c.kk = v3_mul_128(k, k, &of);
-      if (of) {
-        atomicOr(&a.ctr->overflow, 8u);
-        continue;
+  for (;;) {
+    // hand new candidates to idle lanes
+    while (!drained) {
+      const u32 idle = __ballot_sync(0xffffffffu, !active);
+      if (!idle) break;
+      if (chunk_pos >= chunk_end) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(&a.ctr->class_next, (u64)kClassChunk);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) {
+          drained = true;
+          break;
+        }
+        chunk_pos = base;
+        chunk_end = min(base + (u64)kClassChunk, n);
       }
-    } else if (e.kind == KIND_AP) {
-      c.d = V3{{e.d_lo, e.d_hi, 0}};
+      const u32 rank = __popc(idle & lt);
+      const u32 take = (u32)min((u64)__popc(idle), chunk_end - chunk_pos);
+      if (!active && rank < take) active = lane_init(st, a, chunk_pos + rank);
+      chunk_pos += take;
     }
-    const int depth = chain_depth_thr(c, it.mode, it.threshold, it.cap,
-                                      e.two_pass != 0, &imad, &nval);
-    if (depth >= 0) emit_out(a, item, (v << 8) | (u64)min((u32)depth, 255u));
+    if (__ballot_sync(0xffffffffu, active) == 0) break;
+    if (active) {
+      ++nval;
+      const bool pass = sprp_step(chain_value(st.c, st.t), st.bi, &imad);
+      if (st.phase == 0) {
+        if (pass && st.t + 1 < st.lim) {
+          ++st.t;
+        } else {
+          st.d2 = pass ? st.lim : st.t;
+          active = lane_decide(st, a);
+        }
+      } else {
+        if (!pass) {
+          lane_final(st, a, st.t);
+          active = false;
+        } else if (st.bi < 6) {
+          ++st.bi;
+        } else if (st.t + 1 < st.d2) {
+          ++st.t;
+          st.bi = 1;
+        } else {
+          lane_final(st, a, st.d2);
+          active = false;
+        }
+      }
+    }
   }
   // one atomic per warp for the work counters
   u64 s1 = imad, s2 = nval;
@@ -205,8 +319,11 @@ __global__ void k_xq(const DevEngine* engines, const DevItem* items,
   }
 }
 
-// Exclusive scan of the per-item counts (one CTA).
-__global__ void k_scan(const u32* count, u32 n, u64* off) {
+// Exclusive scan of the per-item counts (one CTA).  With n_dev set, the
+// count is read from device memory (graph replays of varying sizes).
+__global__ void k_scan(const u32* count, u32 n, u64* off,
+                       const u32* n_dev = nullptr) {
+  if (n_dev) n = *n_dev;
   __shared__ u64 s_carry;
   __shared__ u64 s_warp[kBlock / 32];
   if (threadIdx.x == 0) s_carry = 0;
@@ -247,6 +364,64 @@ __global__ void k_scatter(const OutRec* out, const DevCounters* ctr,
     const u32 p = atomicAdd(fill + r.item, 1u);
     sorted[off[r.item] + p] = r.packed;
   }
+}
+
+// Buckets for ordering: every item's entries are split by key range into
+// nb = ceil(count / kBucketFill) buckets (the entries of one interval are
+// spread over its span, so a bucket holds about kBucketFill of them), and
+// each bucket is then sorted on its own (k_sort_seg).  nb[i] per item:
+__global__ void k_bucket_nb(const u32* count, u32 n, u32* nb) {
+  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x)
+    nb[i] = count[i] ? (count[i] + kBucketFill - 1) / kBucketFill : 0;
+}
+
+__device__ __forceinline__ u32 bucket_of(const OutRec& r, const DevItem* items,
+                                         const DevEngine* engines,
+                                         const u64* bucket_base,
+                                         const u32* nb) {
+  const DevItem it = items[r.item];
+  const u64 span = (it.mode == MODE_DENSE)
+                       ? it.U
+                       : it.U * engines[it.engine].M;  // keys are below U*M
+  const u32 k = nb[r.item];
+  const u64 key = r.packed >> 8;
+  u64 b = (u64)(((u128)key * k) / (span ? span : 1));
+  if (b >= k) b = k - 1;
+  return (u32)(bucket_base[r.item] + b);
+}
+
+__global__ void k_bucket_count(const OutRec* out, const DevCounters* ctr,
+                               u64 out_cap, const DevItem* items,
+                               const DevEngine* engines,
+                               const u64* bucket_base, const u32* nb,
+                               u32* bcount) {
+  u64 n = ctr->nout;
+  if (n > out_cap) n = out_cap;
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (u64)gridDim.x * blockDim.x)
+    atomicAdd(bcount + bucket_of(out[i], items, engines, bucket_base, nb), 1u);
+}
+
+__global__ void k_bucket_scatter(const OutRec* out, const DevCounters* ctr,
+                                 u64 out_cap, const DevItem* items,
+                                 const DevEngine* engines,
+                                 const u64* bucket_base, const u32* nb,
+                                 const u64* boff, u32* bfill, u64* sorted) {
+  u64 n = ctr->nout;
+  if (n > out_cap) n = out_cap;
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (u64)gridDim.x * blockDim.x) {
+    const OutRec r = out[i];
+    const u32 b = bucket_of(r, items, engines, bucket_base, nb);
+    sorted[boff[b] + atomicAdd(bfill + b, 1u)] = r.packed;
+  }
+}
+
+// The bucket count, for k_sort_seg's device-side segment count.
+__global__ void k_bucket_total(const u64* bucket_base, u32 nitems,
+                               u32* nbuckets) {
+  *nbuckets = (u32)bucket_base[nitems];
 }
 
 // Bitonic sort of buf[0, npow) ascending, npow a power of two, by one CTA.

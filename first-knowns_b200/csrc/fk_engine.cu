@@ -435,6 +435,11 @@ static fk_status build_engine(fk_engine* e) {
   if ((st = upload(e, sbits, &d.sbits))) return st;
   d.NPm = NPm;
   d.use_mark = e->use_mark ? 1 : 0;
+  {
+    u32 w = kNS;
+    while (w < NPm && e->sieve[w] < (u32)(kSeg / 16)) ++w;
+    d.NPw = w;
+  }
   if ((st = upload(e, minv_all, &d.minv_all))) return st;
   if ((st = upload(e, gaux, &d.gaux))) return st;
   if ((st = upload(e, glist, &d.glist))) return st;
@@ -518,6 +523,8 @@ struct fk_batch {
   DevBuf<OutRec> d_out;
   DevBuf<u32> d_item_count, d_item_fill;
   DevBuf<u64> d_item_off, d_sorted, d_scratch;
+  DevBuf<u32> d_nb, d_bcount, d_bfill, d_nbuckets;
+  DevBuf<u64> d_bbase, d_boff;
   DevBuf<unsigned long long> d_task_ctr;
   DevBuf<u32> d_nitems;
   DevCounters* d_ctr = nullptr;
@@ -595,6 +602,8 @@ static void batch_free(fk_batch* b) {
   b->d_xq.release(); b->d_cand_key.release(); b->d_cand_item.release();
   b->d_out.release(); b->d_item_count.release(); b->d_item_fill.release();
   b->d_item_off.release(); b->d_sorted.release(); b->d_scratch.release();
+  b->d_nb.release(); b->d_bcount.release(); b->d_bfill.release();
+  b->d_nbuckets.release(); b->d_bbase.release(); b->d_boff.release();
   b->d_task_ctr.release(); b->d_nitems.release();
   for (auto& f : b->fam) { f.d_idx.release(); f.d_prefix.release(); }
   b->h_items.release(); b->h_ctr.release(); b->h_off.release();
@@ -750,6 +759,15 @@ static fk_status expand(fk_batch* b, const fk_item* items, u64 nitems) {
   if ((st = b->d_item_count.ensure(ni + 1))) return st;
   if ((st = b->d_item_fill.ensure(ni + 1))) return st;
   if ((st = b->d_item_off.ensure(ni + 2))) return st;
+  if ((st = b->d_nb.ensure(ni + 1))) return st;
+  if ((st = b->d_bbase.ensure(ni + 2))) return st;
+  if ((st = b->d_nbuckets.ensure(4))) return st;
+  {
+    const u64 nbk = b->out_cap / kBucketFill + ni + 2;
+    if ((st = b->d_bcount.ensure(nbk))) return st;
+    if ((st = b->d_bfill.ensure(nbk))) return st;
+    if ((st = b->d_boff.ensure(nbk + 1))) return st;
+  }
   if ((st = b->h_items.ensure(ni + 1))) return st;
   if ((st = b->h_off.ensure(ni + 2))) return st;
   if ((st = b->d_dense.ensure(b->dense_idx.size() + 1))) return st;
@@ -780,7 +798,7 @@ static fk_status enqueue(fk_batch* b, bool capturing = false) {
   FK_CUDA(cudaMemsetAsync(b->d_item_count.p, 0, (ni + 1) * sizeof(u32), s));
   FK_CUDA(cudaMemsetAsync(b->d_item_fill.p, 0, (ni + 1) * sizeof(u32), s));
   FK_CUDA(record(b->ev[0], s, capturing));
-  u64 nl = 4;  // classify, scan, scatter, sort
+  u64 nl = 4;  // classify, scan, bucket scatter, sort
   if (!b->sieve_idx.empty()) {
     ++nl;
     dim3 g(64, (u32)std::min<size_t>(b->sieve_idx.size(), 65535));
@@ -845,12 +863,25 @@ static fk_status enqueue(fk_batch* b, bool capturing = false) {
   c.item_count = b->d_item_count.p;
   k_classify<<<b->nsm * 8, kBlock, 0, s>>>(c);
   FK_CUDA(record(b->ev[2], s, capturing));
+  // order: per-item counts -> per-item buckets by key range -> bucket
+  // counts -> scatter -> every bucket sorted in shared memory
+  const u64 nbk_cap = b->d_bcount.cap;
+  FK_CUDA(cudaMemsetAsync(b->d_bcount.p, 0, nbk_cap * sizeof(u32), s));
+  FK_CUDA(cudaMemsetAsync(b->d_bfill.p, 0, nbk_cap * sizeof(u32), s));
   k_scan<<<1, kBlock, 0, s>>>(b->d_item_count.p, ni, b->d_item_off.p);
-  k_scatter<<<b->nsm * 2, kBlock, 0, s>>>(b->d_out.p, b->d_ctr, b->out_cap,
-                                          b->d_item_off.p, b->d_item_fill.p,
-                                          b->d_sorted.p);
-  k_sort_seg<<<(u32)std::min<u64>(std::max<u32>(ni, 1), (u64)b->nsm * 4), kBlock, 0, s>>>(
-      b->d_sorted.p, b->d_item_off.p, b->d_nitems.p, b->d_scratch.p);
+  k_bucket_nb<<<b->nsm, kBlock, 0, s>>>(b->d_item_count.p, ni, b->d_nb.p);
+  k_scan<<<1, kBlock, 0, s>>>(b->d_nb.p, ni, b->d_bbase.p);
+  k_bucket_total<<<1, 1, 0, s>>>(b->d_bbase.p, ni, b->d_nbuckets.p);
+  k_bucket_count<<<b->nsm * 2, kBlock, 0, s>>>(
+      b->d_out.p, b->d_ctr, b->out_cap, b->d_items.p, b->d_engines,
+      b->d_bbase.p, b->d_nb.p, b->d_bcount.p);
+  k_scan<<<1, kBlock, 0, s>>>(b->d_bcount.p, 0u, b->d_boff.p, b->d_nbuckets.p);
+  k_bucket_scatter<<<b->nsm * 2, kBlock, 0, s>>>(
+      b->d_out.p, b->d_ctr, b->out_cap, b->d_items.p, b->d_engines,
+      b->d_bbase.p, b->d_nb.p, b->d_boff.p, b->d_bfill.p, b->d_sorted.p);
+  k_sort_seg<<<b->nsm * 4, kBlock, 0, s>>>(b->d_sorted.p, b->d_boff.p,
+                                           b->d_nbuckets.p, b->d_scratch.p);
+  nl += 6;
   FK_CUDA(cudaGetLastError());
   FK_CUDA(record(b->ev[3], s, capturing));
   FK_CUDA(cudaMemcpyAsync(b->h_ctr.p, b->d_ctr, sizeof(DevCounters),
@@ -948,6 +979,10 @@ static fk_status collect(fk_batch* b) {
     if ((st = b->d_out.ensure(need))) return st;
     if ((st = b->d_sorted.ensure(need))) return st;
     if ((st = b->d_scratch.ensure(2 * need))) return st;
+    const u64 nbk = need / kBucketFill + b->items.size() + 2;
+    if ((st = b->d_bcount.ensure(nbk))) return st;
+    if ((st = b->d_bfill.ensure(nbk))) return st;
+    if ((st = b->d_boff.ensure(nbk + 1))) return st;
     b->cand_cap = b->out_cap = need;
     return set_err(FK_ERR_OVERFLOW, "candidate buffer overflow (grown; rerun)");
   }

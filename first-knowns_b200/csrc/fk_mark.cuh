@@ -200,8 +200,30 @@ __global__ void __launch_bounds__(kBlock, 2) k_mark(SieveArgs a) {
         for (int k = 0; k < kSeg / 16 / kBlock; ++k) b4[tid + k * kBlock] = z;
       }
       __syncthreads();
-      // (b) mark
-      for (u32 i = e.NS + tid; i < e.NPm; i += kBlock) {
+      // (b) mark.  Primes below NPw (at least 16 hits per residue and
+      // segment) one warp each, the lanes splitting every progression
+      // (stride 32q), warps taking primes round robin so the heavy small
+      // primes spread over all warps; larger primes one thread each.
+      {
+        const u32 lane = tid & 31, wid = tid >> 5;
+        for (u32 i = e.NS + wid; i < e.NPw; i += kBlock / 32) {
+          const PrimeRec pr = e.recs[i];
+          const u32 q = pr.q;
+          u32 off = fk_bmod(useg, q, pr.magic) + S.s16[i - e.NS];
+          off = min(off, off - q);
+          const u32 ga = __ldg(e.gaux + i);
+          const u32 go = ga & 0x00FFFFFFu, gc = ga >> 24;
+          for (u32 c = 0; c < gc; ++c) {
+            const u32 g = __ldg(e.glist + go + c);
+            const u32 h0 = g >= off ? g - off : g + q - off;
+            for (u32 h = h0 + lane * q; h < seg_len; h += 32 * q) {
+              S.bytes[h] = 1;
+              ++nmark;
+            }
+          }
+        }
+      }
+      for (u32 i = e.NPw + tid; i < e.NPm; i += kBlock) {
         const PrimeRec pr = e.recs[i];
         const u32 q = pr.q;
         u32 off = fk_bmod(useg, q, pr.magic) + S.s16[i - e.NS];

@@ -313,6 +313,52 @@ __device__ bool bases_rest(const Ctx<L>& c, u64* imad) {
   return true;
 }
 
+// One strong test of m to base kMrBases[bi] (bi = 0 is base 2), with the
+// trial division first: the unit of work of the step interpreter in
+// k_classify.  Every base runs the same loop shape -- square, then on a set
+// bit of d multiply by the base (a modular doubling for base 2) -- so lanes
+// testing different bases of same-sized values stay converged.
+template <int L>
+__device__ __forceinline__ bool step_L(const u64* m, int bi, u64* imad) {
+  const int t = trial_small<L>(m);
+  if (t != 2) return t == 1;
+  Ctx<L> c;
+  ctx_init<L>(c, m);
+  u64 at[L];
+  bool is2 = bi == 0;
+  if (!is2) {
+    u64 a = kMrBases[bi];
+    if (L == 1 && c.m[0] <= a) {
+      a %= c.m[0];
+      if (a == 0) return true;  // huntlib skips a zero base
+    }
+    u64 r2m[L], av[L];
+#pragma unroll
+    for (int i = 0; i < L; ++i) { r2m[i] = c.one[i]; av[i] = 0; }
+    for (int i = 0; i < 64 * L; ++i) mod_double<L>(r2m, c.m);
+    av[0] = a;
+    mont_mul<L>(at, av, r2m, c.m, c.minv);  // a * R mod m
+  }
+  *imad += imad_per_base<L>(c);
+  u64 x[L];
+#pragma unroll
+  for (int i = 0; i < L; ++i) x[i] = c.one[i];
+  for (int b = c.dtop; b >= 0; --b) {
+    mont_mul<L>(x, x, x, c.m, c.minv);
+    if ((c.d[b >> 6] >> (b & 63)) & 1) {
+      if (is2) mod_double<L>(x, c.m);
+      else mont_mul<L>(x, x, at, c.m, c.minv);
+    }
+  }
+  return strong_tail<L>(c, x);
+}
+
+__device__ __noinline__ bool sprp_step(const V3& v, int bi, u64* imad) {
+  if (v.w[2]) return step_L<3>(v.w, bi, imad);
+  if (v.w[1]) return step_L<2>(v.w, bi, imad);
+  return step_L<1>(v.w, bi, imad);
+}
+
 // which = 0: mr_is_prime, 1: sprp_base2, 2: the six bases after 2 only
 // (callers that already know m passes base 2).
 template <int L>

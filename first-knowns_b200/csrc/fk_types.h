@@ -25,6 +25,8 @@ constexpr int kQcap = 4096;       // per-CTA candidate queue (entries)
 constexpr int kNS = 32;           // pattern primes per chain
 constexpr int kMaxRounds = 64;
 constexpr int kSortSmem = 4096;   // entries a CTA sorts in shared memory
+constexpr int kClassChunk = 128;  // candidates a warp fetches at once
+constexpr int kBucketFill = 1024; // expected entries per ordering bucket
 constexpr int kWarpMode = 512;    // queue below which rounds go warp-wide
 constexpr int kSeg = 32768;       // marking: periods per shared segment
 constexpr int kSegPerTask = 8;    // marking: segments per task
@@ -49,6 +51,7 @@ struct DevEngine {
   // byte map; G lists hold each prime's forbidden residues of the PERIOD
   // u for lane offset 0 (f * (M mod q)^-1 mod q)
   uint32_t NPm, use_mark;
+  uint32_t NPw, pad3;             // primes below NPw are marked warp-wide
   const uint32_t* minv_all;       // [NP] (M mod q)^-1 mod q
   const uint32_t* gaux;           // [NP] offset | count << 24 into glist
   const uint32_t* glist;
@@ -88,6 +91,7 @@ struct DevCounters {
   unsigned long long imad_alg;    // algorithmic IMADs of the SPRP stage
   unsigned long long sprp_values; // values strong-tested
   unsigned long long marks;       // marking-sieve byte marks
+  unsigned long long class_next;  // SPRP stage: next candidate chunk
 };
 
 }  // namespace fk
