@@ -137,7 +137,7 @@ struct fk_engine {
 // stored as u16), at most 8192 of them past the pattern primes.
 static u32 NS_marked_end(const fk_engine* e) {
   u32 i = kNS;
-  while (i < e->sieve.size() && e->sieve[i] < 65536u && i - kNS < 8192u) ++i;
+  while (i < e->sieve.size() && e->sieve[i] < 65536u && i - kNS < (u32)kMarkPrimes) ++i;
   return i;
 }
 
@@ -373,16 +373,37 @@ static fk_status build_engine(fk_engine* e) {
     glist.insert(glist.end(), g.begin(), g.end());
   }
   if (glist.size() >= (1u << 24)) return set_err(FK_ERR_DOMAIN, "glist too large");
+  // ---- marking work list: every (prime, forbidden residue) progression
+  // cut into sub-ranges of at least kMarkHits hits and at most 8 per
+  // segment, ordered by prime so a warp's entries share q and trip counts
+  std::vector<u64> mq;
+  std::vector<u32> mitems;
+  for (u32 i = kNS; i < NPm; ++i) {
+    const u32 q = e->sieve[i];
+    const u32 pi = i - kNS;
+    u32 S = 0, nsub = 1;
+    if (q < (u32)(kSeg / kMarkHits)) {
+      const u32 K = std::max<u32>(kMarkHits, ((u32)kSeg / 8 + q - 1) / q);
+      S = K * q;
+      nsub = ((u32)kSeg + S - 1) / S;
+    }
+    mq.push_back((u64)q | ((u64)((u32)kSeg % q) << 16) | ((u64)S << 32));
+    const u32 go = gaux[i] & 0x00FFFFFFu, gc = gaux[i] >> 24;
+    for (u32 k = 0; k < nsub; ++k)
+      for (u32 c = 0; c < gc; ++c)
+        mitems.push_back(glist[go + c] | (pi << 16) | (k << 29));
+  }
   // cost model, in instructions per post-wheel candidate (one lane-period):
   // both kernels run the same pattern stage; the rounds then test each
   // pattern survivor against every remaining prime until one kills it,
-  // the marking sieve pays one byte store per hit plus, per lane, a
-  // per-segment setup for every marked prime and a per-task shift table
+  // the marking sieve pays about 1.5 instructions per byte mark plus, per
+  // segment, one setup per work entry and an offset step per marked
+  // prime, and per lane (task) the shift of every marked prime
   {
     double s1 = 1.0;
     for (u32 i = 0; i < (u32)kNS && i < NP; ++i)
       s1 *= 1.0 - (double)e->forb[i].size() / e->sieve[i];
-    double tests = 0, surv = 1.0, mark_bit = 0, seg = 0, tail = 0;
+    double tests = 0, surv = 1.0, mark_bit = 0, tail = 0;
     double surv_m = 1.0;
     for (u32 i = kNS; i < NP; ++i) {
       const double kill = (double)e->forb[i].size() / e->sieve[i];
@@ -390,17 +411,17 @@ static fk_status build_engine(fk_engine* e) {
       surv *= 1.0 - kill;
       if (i < NPm) {
         mark_bit += kill;
-        seg += 12.0 + 4.0 * e->forb[i].size();
         surv_m *= 1.0 - kill;
       } else {
         tail += surv_m;
         surv_m *= 1.0 - kill;
       }
     }
+    const double npm = NPm > (u32)kNS ? NPm - kNS : 0;
     e->c_round = 2.5 + 22.0 * s1 * tests;
-    e->c_mark_bit = 2.5 + 2.0 + 4.0 * mark_bit + 22.0 * s1 * tail;
-    e->c_mark_seg = seg + 2048.0;
-    e->c_mark_lane = 15.0 * (NPm > (u32)kNS ? NPm - kNS : 0);
+    e->c_mark_bit = 2.5 + 2.0 + 1.5 * mark_bit + 22.0 * s1 * tail;
+    e->c_mark_seg = 12.0 * mitems.size() + 6.0 * npm + 2048.0;
+    e->c_mark_lane = 25.0 * npm;
     e->use_mark = NPm > (u32)kNS;
     if (p.sieve == 1) e->use_mark = false;
     e->force_mark = p.sieve == 2 && e->use_mark;
@@ -435,14 +456,12 @@ static fk_status build_engine(fk_engine* e) {
   if ((st = upload(e, sbits, &d.sbits))) return st;
   d.NPm = NPm;
   d.use_mark = e->use_mark ? 1 : 0;
-  {
-    u32 w = kNS;
-    while (w < NPm && e->sieve[w] < (u32)(kSeg / 16)) ++w;
-    d.NPw = w;
-  }
+  d.nmitems = (u32)mitems.size();
   if ((st = upload(e, minv_all, &d.minv_all))) return st;
   if ((st = upload(e, gaux, &d.gaux))) return st;
   if ((st = upload(e, glist, &d.glist))) return st;
+  if ((st = upload(e, mq, &d.mq))) return st;
+  if ((st = upload(e, mitems, &d.mitems))) return st;
   return FK_OK;
 }
 
@@ -549,6 +568,7 @@ struct fk_batch {
 };
 
 static const int kOccupancy = 2;
+static const int kMarkOccupancy = 3;
 
 static fk_status batch_init(fk_batch* b, fk_engine* const* engines,
                             u32 nengines) {
@@ -828,7 +848,7 @@ static fk_status enqueue(fk_batch* b, bool capturing = false) {
     a.cand_cap = b->cand_cap;
     a.ctr = b->d_ctr;
     a.task_ctr = b->d_task_ctr.p + f;
-    const u64 grid = std::min<u64>(a.ntask, (u64)b->nsm * kOccupancy);
+    const u64 grid = std::min<u64>(a.ntask, (u64)b->nsm * (F.mark ? kMarkOccupancy : kOccupancy));
     ++nl;
     const u32 P0 = F.P0;
     if (F.mark) {

@@ -6,15 +6,21 @@
 // lanes are therefore sieved the Eratosthenes way instead: one CTA owns one
 // lane over kSeg * kSegPerTask consecutive periods, and per segment of
 // kSeg periods it
-//   (a) ORs the compile-time pattern primes into a 512-word bitmap (the
-//       stage-1a pattern sieve of fk_sieve.cuh, two words per thread),
-//   (b) marks every other prime below 2^16 into a kSeg-byte shared map:
-//       for each (prime, forbidden residue) the hits are an arithmetic
-//       progression of step q in u, written with plain byte stores (a mark
-//       is idempotent, so there is no read-modify-write and no atomic), and
+//   (a) ORs the compile-time pattern primes into two words per thread
+//       (the stage-1a pattern sieve of fk_sieve.cuh),
+//   (b) marks every other prime below 2^16 into a kSeg-byte shared map.
+//       Each (prime, forbidden residue) progression of step q is one or
+//       more work entries of at least kMarkHits hits, built once per
+//       engine and ordered by prime; the threads take the entries round
+//       robin, so the heavy small primes spread over every warp and a
+//       warp's entries share q and trip count.  Marks are plain byte
+//       stores (a mark is idempotent: no read-modify-write, no atomic),
+//       four per loop trip, and
 //   (c) extracts the periods that neither marked, tests any primes beyond
 //       the marked range one by one, and appends the survivors to the
 //       candidate list.
+// Each prime's first hit offset lives in shared memory and steps by the
+// tabulated kSeg mod q from one segment to the next.
 // This is the reference AP engine's bitmap marking (primorial-ap/ap_gpu.py:
 // 204-369: tabulated small primes, shared-memory marks for mid primes,
 // global atomics for the rest) re-laid out per lane, so no mark needs an
@@ -26,8 +32,9 @@ namespace fk {
 
 struct MarkSmem {
   unsigned char bytes[kSeg];
-  u64 patw[kSeg / 64];
-  unsigned short s16[8192];
+  unsigned short off16[kMarkPrimes];  // first hit offset of each marked prime
+  u32 ph[kNS];                        // pattern phase at the segment start
+  u32 lsh[kNS];                       // the lane's shift per pattern prime
   u32 warp[kBlock / 32];
   u32 minv[kNS];
   u32 sbits[512];
@@ -39,22 +46,32 @@ struct MarkSmem {
   unsigned long long mbar;
 };
 
+// The two pattern words of thread t in a segment (periods 128t and
+// 128t + 64 from the segment start), from the segment's phases in shared
+// memory: each prime's table index is rebuilt on the fly with a
+// compile-time modulus, so no per-prime phase occupies a register while
+// the segment is marked.
 template <int P0, int I, int NS>
-struct PatSkip {
-  // advance every phase by a compile-time number of periods
-  template <u32 STEP>
-  static __device__ __forceinline__ void skip(u32* rho) {
+struct PatSeg {
+  static __device__ __forceinline__ void words(const u64* __restrict__ spat,
+                                               const u32* ph, u32 t128,
+                                               u64& acc0, u64& acc1) {
     constexpr u32 q = fk_nth_prime(P0 + I);
-    constexpr u32 st = STEP % q;
-    const u32 a = rho[I] + st;
-    rho[I] = min(a, a - q);
-    PatSkip<P0, I + 1, NS>::template skip<STEP>(rho);
+    constexpr u32 off = fk_pat_prefix(P0, I);
+    constexpr u32 st = 64u % q;
+    u32 r = ph[I] + t128 % q;
+    r = min(r, r - q);
+    acc0 |= spat[off + r];
+    u32 r2 = r + st;
+    r2 = min(r2, r2 - q);
+    acc1 |= spat[off + r2];
+    PatSeg<P0, I + 1, NS>::words(spat, ph, t128, acc0, acc1);
   }
 };
 template <int P0, int NS>
-struct PatSkip<P0, NS, NS> {
-  template <u32 STEP>
-  static __device__ __forceinline__ void skip(u32*) {}
+struct PatSeg<P0, NS, NS> {
+  static __device__ __forceinline__ void words(const u64*, const u32*, u32,
+                                               u64&, u64&) {}
 };
 
 // Stage an engine's pattern table into shared memory with a bulk async
@@ -114,7 +131,7 @@ __device__ __forceinline__ bool tail_alive(u64 v, const DevEngine& e,
 }
 
 template <int P0>
-__global__ void __launch_bounds__(kBlock, 2) k_mark(SieveArgs a) {
+__global__ void __launch_bounds__(kBlock, 3) k_mark(SieveArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   u64* spat = reinterpret_cast<u64*>(smem_raw);
   MarkSmem& S = *reinterpret_cast<MarkSmem*>(smem_raw + pat_bytes<P0>());
@@ -168,30 +185,34 @@ __global__ void __launch_bounds__(kBlock, 2) k_mark(SieveArgs a) {
     const u64 R = e.lanes[lane];
     const u64 u_start = chunk * (u64)(kSeg * kSegPerTask);
     const u64 u_end = min((u64)it.U, u_start + (u64)(kSeg * kSegPerTask));
-    // the lane's shift for every marked prime
-    for (u32 i = e.NS + tid; i < e.NPm; i += kBlock) {
-      const PrimeRec pr = e.recs[i];
-      const u32 rq = fk_bmod(R, pr.q, pr.magic);
-      u32 x = xq[i] + rq;
+    const u32 npm = e.NPm - e.NS;
+    // the lane's shift and first-segment phase for every pattern prime
+    if (tid < kNS) {
+      const PrimeRec pr = e.recs[tid];
+      u32 x = xq[tid] + fk_bmod(R, pr.q, pr.magic);
       x = min(x, x - pr.q);
-      S.s16[i - e.NS] =
-          (unsigned short)fk_mulmod(x, __ldg(e.minv_all + i), pr.q, pr.magic);
+      const u32 sh = fk_mulmod(x, S.minv[tid], pr.q, pr.magic);
+      S.lsh[tid] = sh;
+      u32 p = fk_bmod(u_start, pr.q, pr.magic) + sh;
+      S.ph[tid] = min(p, p - pr.q);
     }
-    u32 rho[kNS];
-    Pat<P0, 0, kNS>::setup(rho, R, u_start + 128ull * tid, xq, S.minv);
+    // the first hit offset of every marked prime in the first segment
+    for (u32 pi = tid; pi < npm; pi += kBlock) {
+      const u32 i = e.NS + pi;
+      const PrimeRec pr = e.recs[i];
+      u32 x = xq[i] + fk_bmod(R, pr.q, pr.magic);
+      x = min(x, x - pr.q);
+      const u32 sh = fk_mulmod(x, __ldg(e.minv_all + i), pr.q, pr.magic);
+      u32 o = fk_bmod(u_start, pr.q, pr.magic) + sh;
+      S.off16[pi] = (unsigned short)min(o, o - pr.q);
+    }
     __syncthreads();
     for (u64 useg = u_start; useg < u_end; useg += kSeg) {
       const u32 seg_len = (u32)min((u64)kSeg, u_end - useg);
-      // (a) pattern words 2*tid and 2*tid + 1
-      {
-        u64 acc0 = 0, acc1 = 0;
-        Pat<P0, 0, kNS>::word(spat, rho, acc0);
-        Pat<P0, 0, kNS>::word(spat, rho, acc1);
-        PatSkip<P0, 0, kNS>::template skip<(u32)(kSeg - 128)>(rho);
-        S.patw[2 * tid] = acc0;
-        S.patw[2 * tid + 1] = acc1;
-        nword += 2;
-      }
+      // (a) the pattern words 2*tid and 2*tid + 1
+      u64 acc0 = 0, acc1 = 0;
+      PatSeg<P0, 0, kNS>::words(spat, S.ph, 128u * (u32)tid, acc0, acc1);
+      nword += 2;
       // zero the byte map
       {
         uint4* b4 = reinterpret_cast<uint4*>(S.bytes);
@@ -200,46 +221,54 @@ __global__ void __launch_bounds__(kBlock, 2) k_mark(SieveArgs a) {
         for (int k = 0; k < kSeg / 16 / kBlock; ++k) b4[tid + k * kBlock] = z;
       }
       __syncthreads();
-      // (b) mark.  Primes below NPw (at least 16 hits per residue and
-      // segment) one warp each, the lanes splitting every progression
-      // (stride 32q), warps taking primes round robin so the heavy small
-      // primes spread over all warps; larger primes one thread each.
+      // (b) mark: the work entries round robin over the threads, the next
+      // entry's load in flight while this one's progression is written
       {
-        const u32 lane = tid & 31, wid = tid >> 5;
-        for (u32 i = e.NS + wid; i < e.NPw; i += kBlock / 32) {
-          const PrimeRec pr = e.recs[i];
-          const u32 q = pr.q;
-          u32 off = fk_bmod(useg, q, pr.magic) + S.s16[i - e.NS];
-          off = min(off, off - q);
-          const u32 ga = __ldg(e.gaux + i);
-          const u32 go = ga & 0x00FFFFFFu, gc = ga >> 24;
-          for (u32 c = 0; c < gc; ++c) {
-            const u32 g = __ldg(e.glist + go + c);
-            const u32 h0 = g >= off ? g - off : g + q - off;
-            for (u32 h = h0 + lane * q; h < seg_len; h += 32 * q) {
-              S.bytes[h] = 1;
-              ++nmark;
-            }
+        const u32 nm = e.nmitems;
+        const u32* __restrict__ mit = e.mitems;
+        const u64* __restrict__ mqt = reinterpret_cast<const u64*>(e.mq);
+        unsigned char* __restrict__ B = S.bytes;
+        u32 cnt = 0;
+        u32 i = tid;
+        u32 w = i < nm ? __ldg(mit + i) : 0u;
+        while (i < nm) {
+          const u32 inext = i + kBlock;
+          const u32 wn = inext < nm ? __ldg(mit + inext) : 0u;
+          const u32 g = w & 0xFFFFu, pi = (w >> 16) & 0x1FFFu, k = w >> 29;
+          const u64 m = __ldg(mqt + pi);
+          const u32 q = (u32)m & 0xFFFFu, sl = (u32)(m >> 32);
+          const u32 off = S.off16[pi];
+          u32 h = (g >= off ? g - off : g + q - off) + k * sl;
+          const u32 end = sl ? min(seg_len, (k + 1) * sl) : seg_len;
+          const u32 q2 = 2 * q, q3 = 3 * q, q4 = 4 * q;
+          for (; h + q3 < end; h += q4, cnt += 4) {
+            B[h] = 1;
+            B[h + q] = 1;
+            B[h + q2] = 1;
+            B[h + q3] = 1;
           }
+          for (; h < end; h += q, ++cnt) B[h] = 1;
+          i = inext;
+          w = wn;
         }
-      }
-      for (u32 i = e.NPw + tid; i < e.NPm; i += kBlock) {
-        const PrimeRec pr = e.recs[i];
-        const u32 q = pr.q;
-        u32 off = fk_bmod(useg, q, pr.magic) + S.s16[i - e.NS];
-        off = min(off, off - q);
-        const u32 ga = __ldg(e.gaux + i);
-        const u32 go = ga & 0x00FFFFFFu, gc = ga >> 24;
-        for (u32 c = 0; c < gc; ++c) {
-          const u32 g = __ldg(e.glist + go + c);
-          u32 h = g >= off ? g - off : g + q - off;
-          for (; h < seg_len; h += q) {
-            S.bytes[h] = 1;
-            ++nmark;
-          }
-        }
+        nmark += cnt;
       }
       __syncthreads();
+      // advance the offsets and phases to the next segment (nothing below
+      // reads them before the next segment's barrier)
+      if (useg + kSeg < u_end) {
+        for (u32 pi = tid; pi < npm; pi += kBlock) {
+          const u64 m = __ldg(reinterpret_cast<const u64*>(e.mq) + pi);
+          const u32 q = (u32)m & 0xFFFFu;
+          const u32 o = S.off16[pi] + (((u32)m >> 16) & 0xFFFFu);
+          S.off16[pi] = (unsigned short)min(o, o - q);
+        }
+        if (tid < kNS) {
+          const PrimeRec pr = e.recs[tid];
+          const u32 p = S.ph[tid] + (u32)kSeg % pr.q;
+          S.ph[tid] = min(p, p - pr.q);
+        }
+      }
       // (c) extract
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
@@ -259,7 +288,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_mark(SieveArgs a) {
         if (uw == 0 && R < it.lo_off) valid &= ~1ull;
         if (it.U - uw <= 64 && R >= it.hi_last)
           valid &= ~(1ull << (it.U - uw - 1));
-        u64 surv = ~S.patw[w] & ~m & valid;
+        u64 surv = ~(k ? acc1 : acc0) & ~m & valid;
         while (surv) {
           const int b = __ffsll((long long)surv) - 1;
           surv &= surv - 1;

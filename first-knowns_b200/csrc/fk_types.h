@@ -30,6 +30,9 @@ constexpr int kBucketFill = 1024; // expected entries per ordering bucket
 constexpr int kWarpMode = 512;    // queue below which rounds go warp-wide
 constexpr int kSeg = 32768;       // marking: periods per shared segment
 constexpr int kSegPerTask = 8;    // marking: segments per task
+constexpr int kMarkPrimes = 6528; // marking: most primes one engine marks
+                                  // (every prime from 7 to 2^16 fits)
+constexpr int kMarkHits = 16;     // marking: least hits per work entry
 
 // Immutable per-engine tables (device-resident for the engine's life).
 struct DevEngine {
@@ -51,10 +54,17 @@ struct DevEngine {
   // byte map; G lists hold each prime's forbidden residues of the PERIOD
   // u for lane offset 0 (f * (M mod q)^-1 mod q)
   uint32_t NPm, use_mark;
-  uint32_t NPw, pad3;             // primes below NPw are marked warp-wide
+  uint32_t nmitems, pad3;         // marking work entries
   const uint32_t* minv_all;       // [NP] (M mod q)^-1 mod q
   const uint32_t* gaux;           // [NP] offset | count << 24 into glist
   const uint32_t* glist;
+  // [NPm - NS] per marked prime: q | (kSeg mod q) << 16 | S << 32, where
+  // S is the length of one work entry's sub-range (a multiple of q; 0 when
+  // one entry covers the whole segment)
+  const uint64_t* mq;
+  // [nmitems] work entries g | (prime - NS) << 16 | sub-range << 29: the
+  // hits u = g (mod q), shifted by the lane, inside sub-range k
+  const uint32_t* mitems;
 };
 
 // One unit of work: a sub-range of one engine's line.

@@ -66,7 +66,9 @@ def main():
         print(f"{args.case} run {r}: {dt * 1e3:.1f} ms wall, sieve "
               f"{st['sieve_ms']:.1f} ms, classify {st['classify_ms']:.1f} ms,"
               f" {sum(x[0].size for x in rows)} hits, {st['launches']} "
-              f"launches", flush=True)
+              f"launches, candidates {st['candidates']}, s1_words "
+              f"{st['s1_words']}, s2_tests {st['s2_tests']}, marks "
+              f"{st['marks']}, sprp_values {st['sprp_values']}", flush=True)
 
 
 if __name__ == "__main__":
