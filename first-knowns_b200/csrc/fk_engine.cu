@@ -196,8 +196,8 @@ static fk_status upload(fk_engine* e, const std::vector<T>& h, const D** dptr,
 
 static u32 pat_bytes_for(u32 P0) {
   switch (P0) {
-    case 3: return pat_bytes<3>();
     case 6: return pat_bytes<6>();
+    case 7: return pat_bytes<7>();
     case 9: return pat_bytes<9>();
     default: return pat_bytes<12>();
   }
@@ -214,9 +214,9 @@ static fk_status build_engine(fk_engine* e) {
   if (e->q2 > (1u << 30))
     return set_err(FK_ERR_DOMAIN, "q2 must be at most 2^30 (Barrett range)");
   u32 P0 = p.p0;
-  if (P0 == 0) P0 = (e->kind == KIND_EULER) ? 6 : (e->kind == KIND_AP ? 6 : 6);
-  if (P0 != 3 && P0 != 6 && P0 != 9 && P0 != 12)
-    return set_err(FK_ERR_DOMAIN, "p0 must be 3, 6, 9 or 12");
+  if (P0 == 0) P0 = 6;
+  if (P0 != 6 && P0 != 7 && P0 != 9 && P0 != 12)
+    return set_err(FK_ERR_DOMAIN, "p0 must be 6, 7, 9 or 12");
   e->P0 = P0;
   const u32 first_pat = fk_nth_prime((int)P0);
   const u32 last_pat = fk_nth_prime((int)P0 + kNS - 1);
@@ -584,7 +584,7 @@ static fk_status batch_init(fk_batch* b, fk_engine* const* engines,
   FK_CUDA(cudaGetDevice(&dev));
   FK_CUDA(cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, dev));
   for (int i = 0; i < 4; ++i) FK_CUDA(cudaEventCreate(&b->ev[i]));
-  const u32 P0s[4] = {3, 6, 9, 12};
+  const u32 P0s[4] = {6, 7, 9, 12};
   for (int f = 0; f < 8; ++f) {
     b->fam[f].P0 = P0s[f & 3];
     b->fam[f].mark = f >= 4;
@@ -594,16 +594,16 @@ static fk_status batch_init(fk_batch* b, fk_engine* const* engines,
   FK_CUDA(b->h_ctr.ensure(1) == FK_OK ? cudaSuccess : cudaErrorMemoryAllocation);
   static bool attrs_done = false;
   if (!attrs_done) {
-    FK_CUDA(cudaFuncSetAttribute(k_sieve<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(pat_bytes<3>() + sizeof(SieveSmem))));
+    FK_CUDA(cudaFuncSetAttribute(k_sieve<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(pat_bytes<7>() + sizeof(SieveSmem))));
     FK_CUDA(cudaFuncSetAttribute(k_sieve<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(pat_bytes<6>() + sizeof(SieveSmem))));
     FK_CUDA(cudaFuncSetAttribute(k_sieve<9>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(pat_bytes<9>() + sizeof(SieveSmem))));
     FK_CUDA(cudaFuncSetAttribute(k_sieve<12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(pat_bytes<12>() + sizeof(SieveSmem))));
-    FK_CUDA(cudaFuncSetAttribute(k_mark<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(pat_bytes<3>() + sizeof(MarkSmem))));
+    FK_CUDA(cudaFuncSetAttribute(k_mark<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(pat_bytes<7>() + sizeof(MarkSmem))));
     FK_CUDA(cudaFuncSetAttribute(k_mark<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(pat_bytes<6>() + sizeof(MarkSmem))));
     FK_CUDA(cudaFuncSetAttribute(k_mark<9>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -635,7 +635,7 @@ static void batch_free(fk_batch* b) {
 }
 
 static int fam_of(u32 P0, bool mark) {
-  return (P0 == 3 ? 0 : P0 == 6 ? 1 : P0 == 9 ? 2 : 3) + (mark ? 4 : 0);
+  return (P0 == 6 ? 0 : P0 == 7 ? 1 : P0 == 9 ? 2 : 3) + (mark ? 4 : 0);
 }
 
 
@@ -854,7 +854,7 @@ static fk_status enqueue(fk_batch* b, bool capturing = false) {
     if (F.mark) {
       const size_t sm = pat_bytes_for(P0) + sizeof(MarkSmem);
       switch (P0) {
-        case 3: k_mark<3><<<(u32)grid, kBlock, sm, s>>>(a); break;
+        case 7: k_mark<7><<<(u32)grid, kBlock, sm, s>>>(a); break;
         case 6: k_mark<6><<<(u32)grid, kBlock, sm, s>>>(a); break;
         case 9: k_mark<9><<<(u32)grid, kBlock, sm, s>>>(a); break;
         default: k_mark<12><<<(u32)grid, kBlock, sm, s>>>(a); break;
@@ -862,7 +862,7 @@ static fk_status enqueue(fk_batch* b, bool capturing = false) {
     } else {
       const size_t sm = pat_bytes_for(P0) + sizeof(SieveSmem);
       switch (P0) {
-        case 3: k_sieve<3><<<(u32)grid, kBlock, sm, s>>>(a); break;
+        case 7: k_sieve<7><<<(u32)grid, kBlock, sm, s>>>(a); break;
         case 6: k_sieve<6><<<(u32)grid, kBlock, sm, s>>>(a); break;
         case 9: k_sieve<9><<<(u32)grid, kBlock, sm, s>>>(a); break;
         default: k_sieve<12><<<(u32)grid, kBlock, sm, s>>>(a); break;

@@ -185,7 +185,7 @@ extern "C" fk_status fk_sieve_noalloc(fk_engine* e, const uint64_t lo[2],
       ce = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (ce != cudaSuccess)
         return set_error(FK_ERR_DEVICE, cudaGetErrorString(ce));
-      for (cudaError_t r : {set_smem_limit<3>(), set_smem_limit<6>(),
+      for (cudaError_t r : {set_smem_limit<7>(), set_smem_limit<6>(),
                             set_smem_limit<9>(), set_smem_limit<12>()})
         if (r != cudaSuccess) return set_error(FK_ERR_DEVICE, cudaGetErrorString(r));
       g_scratch_addr[dev] = static_cast<unsigned char*>(p);
@@ -233,7 +233,7 @@ extern "C" fk_status fk_sieve_noalloc(fk_engine* e, const uint64_t lo[2],
   a.task_ctr = at<unsigned long long>(base, kOffTaskCtr);
   const u32 grid = (u32)(ntask < (u64)nsm * 2 ? ntask : (u64)nsm * 2);
   switch (v.P0) {
-    case 3: k_sieve<3><<<grid, kBlock, pat_bytes<3>() + sizeof(SieveSmem), s>>>(a); break;
+    case 7: k_sieve<7><<<grid, kBlock, pat_bytes<7>() + sizeof(SieveSmem), s>>>(a); break;
     case 6: k_sieve<6><<<grid, kBlock, pat_bytes<6>() + sizeof(SieveSmem), s>>>(a); break;
     case 9: k_sieve<9><<<grid, kBlock, pat_bytes<9>() + sizeof(SieveSmem), s>>>(a); break;
     default: k_sieve<12><<<grid, kBlock, pat_bytes<12>() + sizeof(SieveSmem), s>>>(a); break;

@@ -19,27 +19,47 @@ from fk_workloads import (AP, DICKSON, EULER, engine_key, line_range,
                           rows_to_results)
 
 
-def _p0_for(kind, n):
-    # one pattern family for every engine in a batch (see the sieve
-    # kernel's compile-time pattern primes); 17 is the first pattern prime
-    return 6
+# Pattern families (fk_params.p0): 6 puts 2..13 in the wheel and starts
+# the pattern primes at 17; 7 also folds 17 into the wheel, which drops
+# every position 17 kills (a fraction f/17 of them, f = 17's forbidden
+# residues) at the price of 17x fewer periods per lane.  The wider wheel
+# pays when lanes stay long: at least LONG_PERIODS periods, one segment of
+# the marking sieve, so each lane's per-prime setup is still spread thin.
+P0_NARROW, P0_WIDE = 6, 7
+LONG_PERIODS = 1 << 15
 
 
 class EngineSet:
-    """Device engines keyed by (kind, n, q2, d), created on first use."""
+    """Device engines keyed by (kind, n, q2, d, p0), created on first use."""
 
-    def __init__(self):
+    def __init__(self, wide=True):
         self._engines = {}
         self._order = []
+        self.wide = wide
 
     def get(self, key):
+        if len(key) == 4:
+            key = key + (P0_NARROW,)
         if key not in self._engines:
-            kind, n, q2, d = key
-            self._engines[key] = fk_abi.Engine(kind, n, q2=q2,
-                                               p0=_p0_for(kind, n),
+            kind, n, q2, d, p0 = key
+            self._engines[key] = fk_abi.Engine(kind, n, q2=q2, p0=p0,
                                                d=d or None)
             self._order.append(key)
         return self._engines[key]
+
+    def key_for(self, iv):
+        """The engine an interval runs on: the 17# wheel when its lanes
+        stay at least LONG_PERIODS periods long, else the 13# wheel."""
+        base = engine_key(iv) + (P0_NARROW,)
+        if not self.wide:
+            return base
+        e = self.get(base)
+        lo, hi = line_range(iv, e.W if iv.kind == DICKSON else 1)
+        if hi - lo >= LONG_PERIODS * 17 * e.M:
+            wide = engine_key(iv) + (P0_WIDE,)
+            if hi - lo >= LONG_PERIODS * self.get(wide).M:
+                return wide
+        return base
 
     def index(self, key):
         self.get(key)
@@ -56,7 +76,7 @@ def item_specs(engset, intervals):
     """fk_item specs (engine index, mode, threshold, cap, lo, hi)."""
     specs = []
     for iv in intervals:
-        key = engine_key(iv)
+        key = engset.key_for(iv)
         e = engset.get(key)
         lo, hi = line_range(iv, e.W if iv.kind == DICKSON else 1)
         specs.append((engset.index(key), fk_abi.MODE_HUNT, iv.threshold,
@@ -70,7 +90,7 @@ class BatchEngine:
     def __init__(self, intervals=(), engset=None):
         self.engset = engset or EngineSet()
         for iv in intervals:
-            self.engset.get(engine_key(iv))
+            self.engset.get(self.engset.key_for(iv))
         self._batch = None
         self._nengines = -1
 
@@ -98,7 +118,7 @@ class BatchEngine:
         rows = b.run(specs, graph=graph)
         out = []
         for iv, (off, dep) in zip(intervals, rows):
-            e = self.engset.get(engine_key(iv))
+            e = self.engset.get(self.engset.key_for(iv))
             out.append(rows_to_results(iv, off, dep,
                                        e.W if iv.kind == DICKSON else 1))
         return out
@@ -116,7 +136,7 @@ class BatchEngine:
         rows = self._batch.wait()
         out = []
         for iv, (off, dep) in zip(self._pending, rows):
-            e = self.engset.get(engine_key(iv))
+            e = self.engset.get(self.engset.key_for(iv))
             out.append(rows_to_results(iv, off, dep,
                                        e.W if iv.kind == DICKSON else 1))
         return out
@@ -140,7 +160,7 @@ class PlainEngine:
         """Per interval (offsets, depths) as BatchEngine.run_arrays."""
         out = []
         for iv in intervals:
-            e = self.engset.get(engine_key(iv))
+            e = self.engset.get(self.engset.key_for(iv))
             lo, hi = line_range(iv, e.W if iv.kind == DICKSON else 1)
             out.append(e.hunt(lo, hi, iv.threshold, iv.cap))
         return out
@@ -148,7 +168,7 @@ class PlainEngine:
     def run(self, intervals):
         out = []
         for iv in intervals:
-            e = self.engset.get(engine_key(iv))
+            e = self.engset.get(self.engset.key_for(iv))
             W = e.W if iv.kind == DICKSON else 1
             lo, hi = line_range(iv, W)
             off, dep = e.hunt(lo, hi, iv.threshold, iv.cap)

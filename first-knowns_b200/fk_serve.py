@@ -24,7 +24,6 @@ import time
 import numpy as np
 
 from fk_batch import BatchEngine, EngineSet
-from fk_workloads import engine_key
 
 ENTRY_BYTES = 8 + 4 + 16 + 8 + 16   # candidate key/item, out rec, sorted, scratch
 
@@ -38,7 +37,7 @@ class ServeLoop:
         self.hbm_budget = int(hbm_budget)
 
     def footprint(self, iv):
-        e = self.engset.get(engine_key(iv))
+        e = self.engset.get(self.engset.key_for(iv))
         span = iv.length // (e.W if iv.kind == 1 else 1) + 1
         # wheel density x survival estimate, with the pipeline's headroom
         expect = span * e.L / max(e.M, 1) * 0.05 + 64
@@ -48,7 +47,7 @@ class ServeLoop:
         """requests: [(arrival_s, Interval)] sorted by arrival.  Returns
         (results per request, latency_s per request, stats)."""
         for _, iv in requests:
-            self.engset.get(engine_key(iv))   # tables resident up front
+            self.engset.get(self.engset.key_for(iv))   # tables resident up front
         for s in self.slots:
             s._ensure()
         n = len(requests)

@@ -46,7 +46,7 @@ typedef struct fk_params {
   uint32_t kind;      /* FK_EULER / FK_DICKSON / FK_AP                       */
   uint32_t n;         /* filter: values x^2+x+p for x < n; m = 1..n; AP n     */
   uint32_t q2;        /* sieve depth: primes below q2 (0: 65536)              */
-  uint32_t p0;        /* first pattern-sieve prime index: 3, 6, 9 or 12       *
+  uint32_t p0;        /* first pattern-sieve prime index: 6, 7, 9 or 12       *
                        * (all sieve primes below it are folded into the       *
                        * wheel); 0 picks a default for the kind               */
   uint64_t d_lo, d_hi;/* AP difference (0, 0: the n-th primorial)             */

@@ -24,6 +24,12 @@ def sieve(request):
     return request.param
 
 
+@pytest.fixture(params=[6, 7])
+def p0(request):
+    """The 13# wheel (pattern primes from 17) and the 17# wheel."""
+    return request.param
+
+
 def _engine(kind, n, q2=65536, d=None, sieve="auto", p0=6):
     import fk_abi
     return fk_abi.Engine(kind, n, q2=q2, p0=p0, d=d, sieve=sieve)
@@ -35,8 +41,8 @@ EULER_CASES = [(4, 10 ** 7, 2 * 10 ** 6), (6, 10 ** 12, 3 * 10 ** 7),
 
 
 @pytest.mark.parametrize("n,lo,span", EULER_CASES)
-def test_euler_windows(n, lo, span, sieve):
-    eng = _engine(0, n, sieve=sieve)
+def test_euler_windows(n, lo, span, sieve, p0):
+    eng = _engine(0, n, sieve=sieve, p0=p0)
     got = (eng.sieve(lo, lo + span) + np.uint64(0)).tolist()
     want = oeu.CpuEngine(n, oeu.WHEEL_PRIMES).survivors_pre_mr(lo, lo + span)
     assert [lo + o for o in got] == want
@@ -52,8 +58,8 @@ DICKSON_CASES = [(4, 4096, 10 ** 9, 1 << 20), (7, 65536, 10 ** 13, 1 << 22),
 
 
 @pytest.mark.parametrize("n,q2,jlo,span", DICKSON_CASES)
-def test_dickson_windows(n, q2, jlo, span, sieve):
-    eng = _engine(1, n, q2=q2, sieve=sieve)
+def test_dickson_windows(n, q2, jlo, span, sieve, p0):
+    eng = _engine(1, n, q2=q2, sieve=sieve, p0=p0)
     got = (eng.sieve(jlo, jlo + span) + np.uint64(jlo)).tolist()
     want = odk.CpuEngine(n, q2).survivors_j(jlo, jlo + span).tolist()
     assert got == want and len(want) > 0
@@ -67,8 +73,8 @@ AP_CASES = [(5, 2048, None, 10 ** 8 + 10, 30 * (1 << 18)),
 
 
 @pytest.mark.parametrize("n,q2,d,base,span", AP_CASES)
-def test_ap_windows(n, q2, d, base, span, sieve):
-    eng = _engine(2, n, q2=q2, d=d, sieve=sieve)
+def test_ap_windows(n, q2, d, base, span, sieve, p0):
+    eng = _engine(2, n, q2=q2, d=d, sieve=sieve, p0=p0)
     got = eng.sieve(base, base + span).tolist()
     want = oap.CpuEngine(n, q2, d=d).survivors(base, span).tolist()
     assert got == want and len(want) > 0
