@@ -75,6 +75,9 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--tune-seconds", type=float, default=60.0)
+    ap.add_argument("--no-scores", action="store_true")
     return ap.parse_args()
 
 
@@ -213,6 +216,70 @@ def cpu_pool(workers):
                                   mp_context=mp.get_context("spawn"))
 
 
+# ------------------------------------------------- the reference's scores ---
+
+# The reference's own fingerprinted benchmark windows and its published
+# rates for them on one RTX 4090 (euler-prime-runs/score.py:74-77 and
+# BENCHMARKS.md:107; dickson-ladders/score.py:58 and BENCHMARKS.md:40;
+# primorial-ap/score.py:42-50 and BENCHMARKS.md:37).  These time the
+# pre-primality sieve stream only, as the reference's scores do.
+SCORES = {
+    "euler_score_wide": {"published": 2.37e16, "unit": "p/s"},
+    "dickson_score13": {"published": 1.63e17, "unit": "k/s"},
+    "ap_score": {"published": 4.45e10, "unit": "p/s"},
+}
+
+
+def reference_scores(runs=3):
+    """The three score windows through the reference-API mirrors, timed as
+    the reference's score.py times them (median of `runs` after a warm-up,
+    wall clock around the call, device synchronised), with the frozen
+    survivor count and xor checked."""
+    import numpy as np
+    import ap_gpu
+    import euler_gpu
+    import ladder_gpu
+    out = {}
+
+    def timed(fn):
+        fn()
+        ts, res = [], None
+        for _ in range(runs):
+            t0 = time.perf_counter()
+            res = fn()
+            ts.append(time.perf_counter() - t0)
+        return statistics.median(ts), res
+
+    lo, span = 611 * 10 ** 18, 2 * 10 ** 16
+    eng = euler_gpu.GpuEngine(17)
+    t, s = timed(lambda: eng.survivors_pre_mr(lo, lo + span))
+    xor = 0
+    for p in s:
+        xor ^= p
+    out["euler_score_wide"] = {
+        "value": span / t, "seconds": t,
+        "fingerprint_ok": len(s) == 6996 and xor == 71330844491704598}
+    j0, span = 7 * 10 ** 16, 2 ** 38
+    deng = ladder_gpu.GpuEngine(13, q2=65536)
+    t, s = timed(lambda: deng.survivors_j(j0, j0 + span))
+    out["dickson_score13"] = {
+        "value": span * deng.W / t, "seconds": t,
+        "fingerprint_ok": s.size == 2739 and
+        int(np.bitwise_xor.reduce(s)) == 70000110051605722}
+    base, span = (4 * 10 ** 13 // 30) * 30, 30 * 2 ** 25 * 16
+    aeng = ap_gpu.GpuEngine(16, 65536, launch_u=1 << 25)
+    t, s = timed(lambda: np.concatenate(list(aeng.survivors(base, span))))
+    out["ap_score"] = {
+        "value": span / t, "seconds": t,
+        "fingerprint_ok": s.size == 192 and
+        int(np.bitwise_xor.reduce(s)) == 4046714554}
+    for k, v in out.items():
+        v["unit"] = SCORES[k]["unit"]
+        v["published_rtx4090"] = SCORES[k]["published"]
+        v["ratio_to_published"] = v["value"] / SCORES[k]["published"]
+    return out
+
+
 # ------------------------------------------------------------ reference ---
 
 def bench_reference(args):
@@ -269,6 +336,25 @@ def bench_fk(args):
     eng = BatchEngine(intervals)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
+    # autotune the kernel shape on a 1/16 sample of a different draw (the
+    # same seeded shape, so the setting carries over); every rank tunes
+    # its own GPU, and the plain engine gets the same setting
+    tuning = None
+    if not args.no_tune:
+        import fk_tune
+        sample = W.mixed_batch(max(args.count // 16, 16),
+                               W.SEED + 1000 + rank)
+        tb = BatchEngine(sample, engset=eng.engset)
+        res = fk_tune.tune(tb, sample, budget_s=args.tune_seconds)
+        eng.set_tuning(**res["best"])
+        tuning = {"source": "fk_tune coordinate descent on a 1/16 sample "
+                            "(seed + 1000)",
+                  "setting": res["best"], "trials": len(res["trials"]),
+                  "seconds": round(res["seconds"], 1)}
+        del tb
+    else:
+        tuning = {"source": "defaults", "setting": eng.tuning()}
+
     for _ in range(max(args.warmup, 3)):
         ref_rows = eng.run_arrays(intervals, graph=True)
     torch.cuda.synchronize()
@@ -312,6 +398,7 @@ def bench_fk(args):
     bit_identical = None
     if not args.no_plain:
         pe = PlainEngine(eng.engset)
+        pe.set_tuning(**tuning["setting"])
         pe.run_arrays(intervals[:64])          # warm
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -323,36 +410,51 @@ def bench_fk(args):
                  "ms_per_step": tp * 1e3,
                  "calls": len(intervals)}
 
-    # rooflines from the device work counters and measured peaks
+    # rooflines from the device work counters and measured peaks, one per
+    # kernel; the dominant one (most device time) is `roofline`
     imad_peak = fk_abi.peak("imad")
-    smem_peak = fk_abi.peak("smem")
+    st_peak = fk_abi.peak("smem_st")
+    st_mean.update({k: statistics.mean(s[k] for s in stats)
+                    for k in ("mark_ms", "rounds_ms")})
     cls_s = st_mean["classify_ms"] * 1e-3
-    sv_s = st_mean["sieve_ms"] * 1e-3
-    imad_rate = st["imad_alg"] / cls_s if cls_s > 0 else 0.0
-    smem_bytes = st["s1_words"] * 32 * 8
-    smem_rate = smem_bytes / sv_s if sv_s > 0 else 0.0
-    roof_cls = {"kernel": "k_classify (device SPRP chains)", "bound": "imad",
-                "achieved": imad_rate / 1e9, "peak": imad_peak / 1e9,
-                "unit": "G int-multiply-adds/s",
-                "frac": imad_rate / imad_peak if imad_peak else None,
-                "algorithmic": "(bits-1)*(4l^2+2l) per strong-test base, "
-                               "l = ceil(bits/32)",
-                "work_per_launch": st["imad_alg"],
-                "traffic": None,
-                "peak_source": "measured on this GPU by fk_peak (32-bit "
-                               "mad.lo/mad.hi chains)"}
-    roof_sv = {"kernel": "k_sieve (pattern sieve + compaction rounds)",
-               "bound": "smem", "achieved": smem_rate / 1e9,
-               "peak": smem_peak / 1e9, "unit": "GB/s",
-               "frac": smem_rate / smem_peak if smem_peak else None,
-               "algorithmic": "8 B pattern word per pattern prime (32) per "
-                              "64 candidates",
-               "work_per_launch": smem_bytes,
-               "s2_prime_tests": st["s2_tests"], "traffic": None,
-               "peak_source": "measured on this GPU by fk_peak (64-bit "
-                              "conflict-free shared loads)"}
-    dominant, secondary = (roof_sv, roof_cls) if sv_s >= cls_s else \
-        (roof_cls, roof_sv)
+    mark_s = st_mean["mark_ms"] * 1e-3
+    rnd_s = st_mean["rounds_ms"] * 1e-3
+
+    def roof(kernel, bound, work, seconds, peak, unit, scale, algo, src):
+        rate = work / seconds if seconds > 0 else 0.0
+        return {"kernel": kernel, "bound": bound, "achieved": rate / scale,
+                "peak": peak / scale, "unit": unit,
+                "frac": rate / peak if peak else None,
+                "algorithmic": algo, "work_per_launch": work,
+                "seconds_per_launch": seconds, "traffic": None,
+                "peak_source": src}
+
+    roofs = {
+        "k_classify": roof(
+            "k_classify (device SPRP chains)", "imad", st["imad_alg"],
+            cls_s, imad_peak, "G int-multiply-adds/s", 1e9,
+            "(bits-1)*(4l^2+2l) per strong-test base, l = ceil(bits/32)",
+            "measured on this GPU by fk_peak (32-bit mad.lo/mad.hi "
+            "chains, 8 per thread)"),
+        "k_mark": roof(
+            "k_mark (marking sieve)", "smem", st["marks"], mark_s, st_peak,
+            "G byte marks/s", 1e9,
+            "one shared-memory byte store per (period, prime, forbidden "
+            "residue) hit",
+            "measured on this GPU by fk_peak (conflict-free st.shared.u8, "
+            "32 lanes)"),
+        "k_sieve": roof(
+            "k_sieve (pattern sieve + compaction rounds)", "imad",
+            9 * st["s2_tests"], rnd_s, imad_peak, "G int-multiply-adds/s",
+            1e9,
+            "9 IMAD per per-candidate prime test (64-bit Barrett residue: "
+            "8, residue product: 1); the pattern stage's 32 shared loads "
+            "per 64 periods ride alongside",
+            "measured on this GPU by fk_peak (32-bit mad.lo/mad.hi "
+            "chains, 8 per thread)"),
+    }
+    times = {"k_classify": cls_s, "k_mark": mark_s, "k_sieve": rnd_s}
+    dominant = roofs[max(times, key=times.get)]
 
     # CPU baseline (rank 0, one GPU): oracle on a bounded sample
     cpu = None
@@ -384,6 +486,10 @@ def bench_fk(args):
                  "arrival_hz": 250.0, "batches": sst["batches"],
                  "device_busy_frac": sst["device_busy_s"] / sst["wall_s"]}
 
+    scores = None
+    if rank == 0 and world == 1 and not args.no_scores:
+        scores = reference_scores()
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT,
@@ -395,9 +501,10 @@ def bench_fk(args):
             "config": {"workload": WORKLOAD, "intervals": args.count,
                        "candidates_per_rank_step": cands,
                        "l2": "flushed between steps (256 MiB write)",
-                       "graph": True, "device_items": st["items"]},
+                       "graph": True, "device_items": st["items"],
+                       "tuning": tuning},
             "roofline": dominant,
-            "roofline_secondary": secondary,
+            "rooflines": roofs,
             "kernel_ms": st_mean,
             "work": {k: st[k] for k in ("candidates", "outputs", "s1_words",
                                        "s2_tests", "marks", "imad_alg",
@@ -411,6 +518,7 @@ def bench_fk(args):
             "bit_identical": bit_identical,
             "cpu_baseline": cpu,
             "serve": serve,
+            "reference_scores": scores,
             "clocks": clk,
             "gpu_launches": int(st["launches"]) * args.steps,
         }

@@ -110,6 +110,17 @@ static std::string u128_str(u128 x) {
 }
 
 // ---------------------------------------------------------------- engine ---
+// The sieve kernels' cost model, in instructions per post-wheel candidate
+// (one lane-period) plus per-segment and per-lane terms, for one bound of
+// the marked primes.
+struct Cost {
+  double round = 0;   // compaction rounds, per lane-period
+  double bit = 0;     // marking, per lane-period
+  double seg = 0;     // marking, per segment
+  double lane = 0;    // marking, per task (one lane's shifts)
+  bool mark = false;  // the marking sieve is available
+};
+
 struct fk_engine {
   fk_params p{};
   u32 kind = 0, n = 0, q2 = 0, P0 = 0;
@@ -123,8 +134,8 @@ struct fk_engine {
   double survival = 1.0;      // expected survival through every sieve prime
   bool use_mark = false;      // long lanes go to the marking sieve
   bool force_mark = false;    // every item goes to the marking sieve
-  double c_round = 0, c_mark_bit = 0, c_mark_seg = 0, c_mark_lane = 0;
-  double test_cost = 0, mark_cost = 0;
+  std::vector<u32> mprefix;   // marking work entries before each marked prime
+  Cost cost;                  // cost model with every prime below 2^16 marked
   DevEngine dev{};
   std::vector<void*> allocs;
   u64 device_bytes = 0;
@@ -199,8 +210,43 @@ static u32 pat_bytes_for(u32 P0) {
     case 6: return pat_bytes<6>();
     case 7: return pat_bytes<7>();
     case 9: return pat_bytes<9>();
-    default: return pat_bytes<12>();
+    default: return pat_bytes<11>();
   }
+}
+
+// Both kernels run the same pattern stage; the rounds then test each
+// pattern survivor against every remaining prime until one kills it; the
+// marking sieve pays about 1.5 instructions per byte mark plus, per
+// segment, one setup per work entry and an offset step per marked prime,
+// and per lane (task) the shift of every marked prime; candidates that
+// survive the marked primes are tested one by one against the rest.
+static Cost engine_cost(const fk_engine* e, u32 NPm) {
+  Cost c;
+  const u32 NP = (u32)e->sieve.size();
+  double s1 = 1.0;
+  for (u32 i = 0; i < (u32)kNS && i < NP; ++i)
+    s1 *= 1.0 - (double)e->forb[i].size() / e->sieve[i];
+  double tests = 0, surv = 1.0, mark_bit = 0, tail = 0, surv_m = 1.0;
+  for (u32 i = kNS; i < NP; ++i) {
+    const double kill = (double)e->forb[i].size() / e->sieve[i];
+    tests += surv;
+    surv *= 1.0 - kill;
+    if (i < NPm) {
+      mark_bit += kill;
+    } else {
+      tail += surv_m;
+    }
+    surv_m *= 1.0 - kill;
+  }
+  const double npm = NPm > (u32)kNS ? NPm - kNS : 0;
+  const double items = NPm > (u32)kNS && !e->mprefix.empty()
+                           ? e->mprefix[NPm - kNS] : 0;
+  c.round = 2.5 + 22.0 * s1 * tests;
+  c.bit = 2.5 + 2.0 + 1.5 * mark_bit + 22.0 * s1 * tail;
+  c.seg = 12.0 * items + 6.0 * npm + 2048.0;
+  c.lane = 25.0 * npm;
+  c.mark = NPm > (u32)kNS;
+  return c;
 }
 
 static fk_status build_engine(fk_engine* e) {
@@ -215,8 +261,8 @@ static fk_status build_engine(fk_engine* e) {
     return set_err(FK_ERR_DOMAIN, "q2 must be at most 2^30 (Barrett range)");
   u32 P0 = p.p0;
   if (P0 == 0) P0 = 6;
-  if (P0 != 6 && P0 != 7 && P0 != 9 && P0 != 12)
-    return set_err(FK_ERR_DOMAIN, "p0 must be 6, 7, 9 or 12");
+  if (P0 != 6 && P0 != 7 && P0 != 9 && P0 != 11)
+    return set_err(FK_ERR_DOMAIN, "p0 must be 6, 7, 9 or 11");
   e->P0 = P0;
   const u32 first_pat = fk_nth_prime((int)P0);
   const u32 last_pat = fk_nth_prime((int)P0 + kNS - 1);
@@ -254,15 +300,19 @@ static fk_status build_engine(fk_engine* e) {
     for (u32 r : f) bad[r] = 1;
     std::vector<u64> nl;
     const u64 cnt = (u64)e->lanes.size() * (q - f.size());
-    if (cnt > (1ull << 22))
+    if (cnt > (1ull << 26))
       return set_err(FK_ERR_DOMAIN, "wheel has too many lanes; use a smaller p0");
     nl.reserve(cnt);
-    for (u64 t = 0; t < q; ++t)
+    // t outer, r inner: every r < M, so the lifts come out ascending
+    const u32 Mq = (u32)(e->M % q);
+    for (u64 t = 0; t < q; ++t) {
+      const u32 tq = (u32)((t * Mq) % q);
       for (u64 r : e->lanes) {
-        const u64 x = r + t * e->M;
-        if (!bad[x % q]) nl.push_back(x);
+        u32 xr = (u32)(r % q) + tq;
+        if (xr >= q) xr -= q;
+        if (!bad[xr]) nl.push_back(r + t * e->M);
       }
-    std::sort(nl.begin(), nl.end());
+    }
     e->lanes.swap(nl);
     e->M *= q;
     e->wheel.push_back(q);
@@ -388,46 +438,17 @@ static fk_status build_engine(fk_engine* e) {
       nsub = ((u32)kSeg + S - 1) / S;
     }
     mq.push_back((u64)q | ((u64)((u32)kSeg % q) << 16) | ((u64)S << 32));
+    e->mprefix.push_back((u32)mitems.size());
     const u32 go = gaux[i] & 0x00FFFFFFu, gc = gaux[i] >> 24;
     for (u32 k = 0; k < nsub; ++k)
       for (u32 c = 0; c < gc; ++c)
         mitems.push_back(glist[go + c] | (pi << 16) | (k << 29));
   }
-  // cost model, in instructions per post-wheel candidate (one lane-period):
-  // both kernels run the same pattern stage; the rounds then test each
-  // pattern survivor against every remaining prime until one kills it,
-  // the marking sieve pays about 1.5 instructions per byte mark plus, per
-  // segment, one setup per work entry and an offset step per marked
-  // prime, and per lane (task) the shift of every marked prime
-  {
-    double s1 = 1.0;
-    for (u32 i = 0; i < (u32)kNS && i < NP; ++i)
-      s1 *= 1.0 - (double)e->forb[i].size() / e->sieve[i];
-    double tests = 0, surv = 1.0, mark_bit = 0, tail = 0;
-    double surv_m = 1.0;
-    for (u32 i = kNS; i < NP; ++i) {
-      const double kill = (double)e->forb[i].size() / e->sieve[i];
-      tests += surv;
-      surv *= 1.0 - kill;
-      if (i < NPm) {
-        mark_bit += kill;
-        surv_m *= 1.0 - kill;
-      } else {
-        tail += surv_m;
-        surv_m *= 1.0 - kill;
-      }
-    }
-    const double npm = NPm > (u32)kNS ? NPm - kNS : 0;
-    e->c_round = 2.5 + 22.0 * s1 * tests;
-    e->c_mark_bit = 2.5 + 2.0 + 1.5 * mark_bit + 22.0 * s1 * tail;
-    e->c_mark_seg = 12.0 * mitems.size() + 6.0 * npm + 2048.0;
-    e->c_mark_lane = 25.0 * npm;
-    e->use_mark = NPm > (u32)kNS;
-    if (p.sieve == 1) e->use_mark = false;
-    e->force_mark = p.sieve == 2 && e->use_mark;
-    e->test_cost = e->c_round;
-    e->mark_cost = e->c_mark_bit;
-  }
+  e->mprefix.push_back((u32)mitems.size());
+  e->cost = engine_cost(e, NPm);
+  e->use_mark = e->cost.mark;
+  if (p.sieve == 1) e->use_mark = false;
+  e->force_mark = p.sieve == 2 && e->use_mark;
   // ---- upload -------------------------------------------------------------
   DevEngine& d = e->dev;
   d.kind = e->kind;
@@ -525,6 +546,9 @@ struct Family {
 struct fk_batch {
   std::vector<fk_engine*> engines;
   DevEngine* d_engines = nullptr;
+  fk_tuning tune{};
+  std::vector<Cost> cost;       // per engine, for this batch's mark_limit
+  std::vector<uint8_t> mark_ok; // per engine: the marking sieve may run
   cudaStream_t stream = nullptr;
   int nsm = 148;
   // host-side item expansion
@@ -558,6 +582,8 @@ struct fk_batch {
   cudaGraphExec_t gexec = nullptr;
   std::vector<u64> graph_key;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t fev[16] = {};     // before / after each family's launch
+  bool fam_ran[8] = {};
   // results
   std::vector<uint64_t> r_start, r_off;
   std::vector<uint8_t> r_depth;
@@ -567,24 +593,48 @@ struct fk_batch {
   u64 h2d = 0, d2h = 0;
 };
 
-static const int kOccupancy = 2;
-static const int kMarkOccupancy = 3;
+static const fk_tuning kDefaultTuning = {2, 3, 2048, (u32)kWarpMode,
+                                         (u32)kSegPerTask, 8, 65536, 1.0f};
+
+// Upload this batch's copy of every engine descriptor with the marked
+// prime range cut at tune.mark_limit, and the matching cost models.
+static fk_status apply_tuning(fk_batch* b) {
+  const u32 ne = (u32)b->engines.size();
+  std::vector<DevEngine> de(ne);
+  b->cost.assign(ne, Cost());
+  b->mark_ok.assign(ne, 0);
+  for (u32 i = 0; i < ne; ++i) {
+    const fk_engine* e = b->engines[i];
+    DevEngine d = e->dev;
+    u32 npm = d.NPm;
+    while (npm > (u32)kNS && e->sieve[npm - 1] >= b->tune.mark_limit) --npm;
+    d.NPm = npm;
+    d.nmitems = npm > (u32)kNS ? e->mprefix[npm - kNS] : 0;
+    b->cost[i] = npm == e->dev.NPm ? e->cost : engine_cost(e, npm);
+    b->mark_ok[i] = e->use_mark && npm > (u32)kNS;
+    d.use_mark = b->mark_ok[i];
+    de[i] = d;
+  }
+  FK_CUDA(cudaMemcpy(b->d_engines, de.data(), sizeof(DevEngine) * ne,
+                     cudaMemcpyHostToDevice));
+  return FK_OK;
+}
 
 static fk_status batch_init(fk_batch* b, fk_engine* const* engines,
                             u32 nengines) {
   b->engines.assign(engines, engines + nengines);
-  std::vector<DevEngine> de(nengines);
-  for (u32 i = 0; i < nengines; ++i) de[i] = engines[i]->dev;
   FK_CUDA(cudaMalloc(&b->d_engines, sizeof(DevEngine) * std::max<u32>(nengines, 1)));
-  FK_CUDA(cudaMemcpy(b->d_engines, de.data(), sizeof(DevEngine) * nengines,
-                     cudaMemcpyHostToDevice));
+  b->tune = kDefaultTuning;
+  fk_status st0 = apply_tuning(b);
+  if (st0) return st0;
   FK_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
   FK_CUDA(cudaMalloc(&b->d_ctr, sizeof(DevCounters)));
   int dev = 0;
   FK_CUDA(cudaGetDevice(&dev));
   FK_CUDA(cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, dev));
   for (int i = 0; i < 4; ++i) FK_CUDA(cudaEventCreate(&b->ev[i]));
-  const u32 P0s[4] = {6, 7, 9, 12};
+  for (int i = 0; i < 16; ++i) FK_CUDA(cudaEventCreate(&b->fev[i]));
+  const u32 P0s[4] = {6, 7, 9, 11};
   for (int f = 0; f < 8; ++f) {
     b->fam[f].P0 = P0s[f & 3];
     b->fam[f].mark = f >= 4;
@@ -600,16 +650,16 @@ static fk_status batch_init(fk_batch* b, fk_engine* const* engines,
                                  (int)(pat_bytes<6>() + sizeof(SieveSmem))));
     FK_CUDA(cudaFuncSetAttribute(k_sieve<9>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(pat_bytes<9>() + sizeof(SieveSmem))));
-    FK_CUDA(cudaFuncSetAttribute(k_sieve<12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(pat_bytes<12>() + sizeof(SieveSmem))));
+    FK_CUDA(cudaFuncSetAttribute(k_sieve<11>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(pat_bytes<11>() + sizeof(SieveSmem))));
     FK_CUDA(cudaFuncSetAttribute(k_mark<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(pat_bytes<7>() + sizeof(MarkSmem))));
     FK_CUDA(cudaFuncSetAttribute(k_mark<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(pat_bytes<6>() + sizeof(MarkSmem))));
     FK_CUDA(cudaFuncSetAttribute(k_mark<9>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(pat_bytes<9>() + sizeof(MarkSmem))));
-    FK_CUDA(cudaFuncSetAttribute(k_mark<12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(pat_bytes<12>() + sizeof(MarkSmem))));
+    FK_CUDA(cudaFuncSetAttribute(k_mark<11>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(pat_bytes<11>() + sizeof(MarkSmem))));
     attrs_done = true;
   }
   return FK_OK;
@@ -631,6 +681,7 @@ static void batch_free(fk_batch* b) {
   if (b->d_ctr) cudaFree(b->d_ctr);
   if (b->d_engines) cudaFree(b->d_engines);
   for (auto& e : b->ev) if (e) cudaEventDestroy(e);
+  for (auto& e : b->fev) if (e) cudaEventDestroy(e);
   if (b->stream) cudaStreamDestroy(b->stream);
 }
 
@@ -659,7 +710,8 @@ static fk_status expand(fk_batch* b, const fk_item* items, u64 nitems) {
   b->dense_idx.clear();
   b->sieve_idx.clear();
   for (auto& f : b->fam) { f.idx.clear(); f.prefix.assign(1, 0); }
-  const u64 target_chains = (u64)b->nsm * kOccupancy * kBlock * 4;
+  const u64 target_chains = (u64)b->nsm * b->tune.chains_per_sm;
+  const u64 seg_task = (u64)kSeg * b->tune.seg_per_task;
   for (u64 ui = 0; ui < nitems; ++ui) {
     const fk_item& it = items[ui];
     if (it.engine >= b->engines.size())
@@ -712,18 +764,18 @@ static fk_status expand(fk_batch* b, const fk_item* items, u64 nitems) {
       const bool last = s0 + U >= periods;
       di.hi_last = last ? (u64)(hi - (base + (u128)(U - 1) * M)) : M;
       bool mark = false;
-      if (e->use_mark) {
+      if (b->mark_ok[it.engine]) {
+        const Cost& c = b->cost[it.engine];
         const double Ud = (double)U;
-        const double rounds = Ud * e->c_round;
-        const double tasks = std::ceil(Ud / ((double)kSeg * kSegPerTask));
+        const double rounds = Ud * c.round;
+        const double tasks = std::ceil(Ud / (double)seg_task);
         const double segs = std::ceil(Ud / kSeg);
-        const double marking = tasks * e->c_mark_lane + segs * e->c_mark_seg +
-                               Ud * e->c_mark_bit;
-        mark = e->force_mark || marking < rounds;
+        const double marking = tasks * c.lane + segs * c.seg + Ud * c.bit;
+        mark = e->force_mark || marking < (double)b->tune.mark_bias * rounds;
       }
       di.marked = mark ? 1 : 0;
       if (mark) {
-        di.nchunk_u = (U + (u64)kSeg * kSegPerTask - 1) / ((u64)kSeg * kSegPerTask);
+        di.nchunk_u = (U + seg_task - 1) / seg_task;
         di.ntask = L * di.nchunk_u;
         di.Tc = 0;
         di.nchunk = 0;
@@ -834,7 +886,9 @@ static fk_status enqueue(fk_batch* b, bool capturing = false) {
   }
   for (int f = 0; f < 8; ++f) {
     Family& F = b->fam[f];
+    b->fam_ran[f] = !F.idx.empty();
     if (F.idx.empty()) continue;
+    FK_CUDA(record(b->fev[2 * f], s, capturing));
     SieveArgs a{};
     a.engines = b->d_engines;
     a.items = b->d_items.p;
@@ -848,7 +902,11 @@ static fk_status enqueue(fk_batch* b, bool capturing = false) {
     a.cand_cap = b->cand_cap;
     a.ctr = b->d_ctr;
     a.task_ctr = b->d_task_ctr.p + f;
-    const u64 grid = std::min<u64>(a.ntask, (u64)b->nsm * (F.mark ? kMarkOccupancy : kOccupancy));
+    a.warp_queue = b->tune.warp_queue;
+    a.seg_per_task = b->tune.seg_per_task;
+    const u64 grid = std::min<u64>(
+        a.ntask, (u64)b->nsm * (F.mark ? b->tune.mark_ctas_per_sm
+                                       : b->tune.sieve_ctas_per_sm));
     ++nl;
     const u32 P0 = F.P0;
     if (F.mark) {
@@ -857,7 +915,7 @@ static fk_status enqueue(fk_batch* b, bool capturing = false) {
         case 7: k_mark<7><<<(u32)grid, kBlock, sm, s>>>(a); break;
         case 6: k_mark<6><<<(u32)grid, kBlock, sm, s>>>(a); break;
         case 9: k_mark<9><<<(u32)grid, kBlock, sm, s>>>(a); break;
-        default: k_mark<12><<<(u32)grid, kBlock, sm, s>>>(a); break;
+        default: k_mark<11><<<(u32)grid, kBlock, sm, s>>>(a); break;
       }
     } else {
       const size_t sm = pat_bytes_for(P0) + sizeof(SieveSmem);
@@ -865,9 +923,10 @@ static fk_status enqueue(fk_batch* b, bool capturing = false) {
         case 7: k_sieve<7><<<(u32)grid, kBlock, sm, s>>>(a); break;
         case 6: k_sieve<6><<<(u32)grid, kBlock, sm, s>>>(a); break;
         case 9: k_sieve<9><<<(u32)grid, kBlock, sm, s>>>(a); break;
-        default: k_sieve<12><<<(u32)grid, kBlock, sm, s>>>(a); break;
+        default: k_sieve<11><<<(u32)grid, kBlock, sm, s>>>(a); break;
       }
     }
+    FK_CUDA(record(b->fev[2 * f + 1], s, capturing));
   }
   FK_CUDA(cudaGetLastError());
   FK_CUDA(record(b->ev[1], s, capturing));
@@ -881,7 +940,7 @@ static fk_status enqueue(fk_batch* b, bool capturing = false) {
   c.out = b->d_out.p;
   c.out_cap = b->out_cap;
   c.item_count = b->d_item_count.p;
-  k_classify<<<b->nsm * 8, kBlock, 0, s>>>(c);
+  k_classify<<<b->nsm * b->tune.classify_ctas_per_sm, kBlock, 0, s>>>(c);
   FK_CUDA(record(b->ev[2], s, capturing));
   // order: per-item counts -> per-item buckets by key range -> bucket
   // counts -> scatter -> every bucket sorted in shared memory
@@ -963,6 +1022,9 @@ static fk_status launch(fk_batch* b, int use_graph) {
   for (auto& f : b->fam) { key.push_back(f.idx.size()); key.push_back(f.prefix.back()); }
   key.push_back((u64)(uintptr_t)b->d_items.p);
   key.push_back((u64)(uintptr_t)b->d_cand_key.p);
+  key.push_back(((u64)b->tune.sieve_ctas_per_sm << 32) | b->tune.mark_ctas_per_sm);
+  key.push_back(((u64)b->tune.warp_queue << 32) | b->tune.seg_per_task);
+  key.push_back(b->tune.classify_ctas_per_sm);
   if (b->gexec == nullptr || key != b->graph_key) {
     if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
     if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
@@ -1237,7 +1299,46 @@ static fk_status stats_of(const fk_batch* b, fk_stats* out) {
   out->sieve_ms = a;
   out->classify_ms = cl;
   out->total_ms = t;
+  for (int f = 0; f < 8; ++f) {
+    if (!b->fam_ran[f]) continue;
+    float x = 0;
+    FK_CUDA(cudaEventElapsedTime(&x, b->fev[2 * f], b->fev[2 * f + 1]));
+    (b->fam[f].mark ? out->mark_ms : out->rounds_ms) += x;
+  }
   return FK_OK;
+}
+
+fk_status fk_batch_set_tuning(fk_batch* b, const fk_tuning* t) {
+  if (!b || !t) return set_err(FK_ERR_ARG, "null argument");
+  if (b->pending) return set_err(FK_ERR_ARG, "a submitted run is pending");
+  fk_tuning n = b->tune;
+  if (t->sieve_ctas_per_sm) n.sieve_ctas_per_sm = t->sieve_ctas_per_sm;
+  if (t->mark_ctas_per_sm) n.mark_ctas_per_sm = t->mark_ctas_per_sm;
+  if (t->chains_per_sm) n.chains_per_sm = t->chains_per_sm;
+  if (t->warp_queue) n.warp_queue = t->warp_queue;
+  if (t->seg_per_task) n.seg_per_task = t->seg_per_task;
+  if (t->classify_ctas_per_sm) n.classify_ctas_per_sm = t->classify_ctas_per_sm;
+  if (t->mark_limit) n.mark_limit = t->mark_limit;
+  if (t->mark_bias > 0.0f) n.mark_bias = t->mark_bias;
+  if (n.sieve_ctas_per_sm > 2 || n.mark_ctas_per_sm > 3 ||
+      n.chains_per_sm < 64 || n.chains_per_sm > 65536 ||
+      n.warp_queue > (u32)kWq || n.seg_per_task > 64 ||
+      n.classify_ctas_per_sm > 32 || n.mark_limit > 65536 ||
+      !(n.mark_bias < 1e6f))
+    return set_err(FK_ERR_DOMAIN, "tuning value out of range");
+  b->tune = n;
+  return apply_tuning(b);
+}
+
+fk_status fk_batch_get_tuning(const fk_batch* b, fk_tuning* out) {
+  if (!b || !out) return set_err(FK_ERR_ARG, "null argument");
+  *out = b->tune;
+  return FK_OK;
+}
+
+fk_status fk_engine_set_tuning(fk_engine* e, const fk_tuning* t) {
+  if (!e || !t) return set_err(FK_ERR_ARG, "null argument");
+  return fk_batch_set_tuning(e->plain, t);
 }
 
 fk_status fk_batch_stats(const fk_batch* b, fk_stats* out) {
@@ -1307,8 +1408,25 @@ __global__ void k_peak_smem(u32 iters, u64* sink) {
   if ((acc0 ^ acc1 ^ acc2 ^ acc3) == 0x1234ull) sink[0] = acc0;
 }
 
+// Shared-memory byte stores: eight independent conflict-free st.shared.u8
+// per thread per trip (lane i of a warp writes bank i).
+__global__ void k_peak_smem_st(u32 iters, u32* sink) {
+  __shared__ __align__(16) unsigned char buf[kBlock * 4 * 8];
+  const u32 base = (u32)__cvta_generic_to_shared(buf) + 4u * threadIdx.x;
+  for (u32 it = 0; it < iters; ++it) {
+#pragma unroll
+    for (u32 k = 0; k < 8; ++k)
+      asm volatile("st.shared.u8 [%0], %1;" ::"r"(base + k * 4u * kBlock),
+                   "r"(it)
+                   : "memory");
+  }
+  __syncthreads();
+  if (buf[threadIdx.x] == 0xA5 && iters == 0) sink[0] = 1;
+}
+
 extern "C" fk_status fk_peak(int which, double* per_second) {
   if (!per_second) return set_err(FK_ERR_ARG, "null argument");
+  if (which < 0 || which > 2) return set_err(FK_ERR_ARG, "which must be 0, 1 or 2");
   int dev = 0, nsm = 0;
   FK_CUDA(cudaGetDevice(&dev));
   FK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -1323,8 +1441,10 @@ extern "C" fk_status fk_peak(int which, double* per_second) {
     FK_CUDA(cudaEventRecord(e0));
     if (which == 0)
       k_peak_imad<<<grid, kBlock>>>(rep + 7, iters, (u32*)sink);
-    else
+    else if (which == 1)
       k_peak_smem<<<grid, kBlock>>>(iters, (u64*)sink);
+    else
+      k_peak_smem_st<<<grid, kBlock>>>(iters, (u32*)sink);
     FK_CUDA(cudaEventRecord(e1));
     FK_CUDA(cudaEventSynchronize(e1));
     float ms = 0;
@@ -1335,8 +1455,9 @@ extern "C" fk_status fk_peak(int which, double* per_second) {
   cudaEventDestroy(e1);
   cudaFree(sink);
   const double threads = (double)grid * kBlock;
-  const double work = which == 0 ? threads * iters * 8.0        // IMADs
-                                 : threads * iters * 4.0 * 8.0; // bytes
+  const double work = which == 0   ? threads * iters * 8.0        // IMADs
+                      : which == 1 ? threads * iters * 4.0 * 8.0  // bytes
+                                   : threads * iters * 8.0;       // stores
   *per_second = work / (best * 1e-3);
   return FK_OK;
 }

@@ -4,7 +4,7 @@
 // candidates alive deep into the prime list, and testing each of them
 // against every remaining prime costs tens of tests per candidate.  Long
 // lanes are therefore sieved the Eratosthenes way instead: one CTA owns one
-// lane over kSeg * kSegPerTask consecutive periods, and per segment of
+// lane over kSeg * seg_per_task consecutive periods, and per segment of
 // kSeg periods it
 //   (a) ORs the compile-time pattern primes into two words per thread
 //       (the stage-1a pattern sieve of fk_sieve.cuh),
@@ -183,9 +183,9 @@ __global__ void __launch_bounds__(kBlock, 3) k_mark(SieveArgs a) {
     const u32 lane = (u32)(tl % e.L);
     const u64 chunk = tl / e.L;
     const u64 R = e.lanes[lane];
-    const u64 u_start = chunk * (u64)(kSeg * kSegPerTask);
-    const u64 u_end = min((u64)it.U, u_start + (u64)(kSeg * kSegPerTask));
-    const u32 npm = e.NPm - e.NS;
+    const u64 u_start = chunk * (u64)kSeg * a.seg_per_task;
+    const u64 u_end = min((u64)it.U, u_start + (u64)kSeg * a.seg_per_task);
+    const u32 npm = e.NPm - e.NS;   // marked primes (the batch's bound)
     // the lane's shift and first-segment phase for every pattern prime
     if (tid < kNS) {
       const PrimeRec pr = e.recs[tid];

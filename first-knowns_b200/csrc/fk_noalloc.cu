@@ -186,7 +186,7 @@ extern "C" fk_status fk_sieve_noalloc(fk_engine* e, const uint64_t lo[2],
       if (ce != cudaSuccess)
         return set_error(FK_ERR_DEVICE, cudaGetErrorString(ce));
       for (cudaError_t r : {set_smem_limit<7>(), set_smem_limit<6>(),
-                            set_smem_limit<9>(), set_smem_limit<12>()})
+                            set_smem_limit<9>(), set_smem_limit<11>()})
         if (r != cudaSuccess) return set_error(FK_ERR_DEVICE, cudaGetErrorString(r));
       g_scratch_addr[dev] = static_cast<unsigned char*>(p);
     }
@@ -231,12 +231,14 @@ extern "C" fk_status fk_sieve_noalloc(fk_engine* e, const uint64_t lo[2],
   a.cand_cap = kMaxCand;
   a.ctr = at<DevCounters>(base, kOffCtr);
   a.task_ctr = at<unsigned long long>(base, kOffTaskCtr);
+  a.warp_queue = kWarpMode;
+  a.seg_per_task = kSegPerTask;
   const u32 grid = (u32)(ntask < (u64)nsm * 2 ? ntask : (u64)nsm * 2);
   switch (v.P0) {
     case 7: k_sieve<7><<<grid, kBlock, pat_bytes<7>() + sizeof(SieveSmem), s>>>(a); break;
     case 6: k_sieve<6><<<grid, kBlock, pat_bytes<6>() + sizeof(SieveSmem), s>>>(a); break;
     case 9: k_sieve<9><<<grid, kBlock, pat_bytes<9>() + sizeof(SieveSmem), s>>>(a); break;
-    default: k_sieve<12><<<grid, kBlock, pat_bytes<12>() + sizeof(SieveSmem), s>>>(a); break;
+    default: k_sieve<11><<<grid, kBlock, pat_bytes<11>() + sizeof(SieveSmem), s>>>(a); break;
   }
   const u64 lo_shift = (u64)(L0 - X0);
   k_na_finish<<<1, kBlock, 0, s>>>(base, reinterpret_cast<u64*>(d_offsets),

@@ -17,12 +17,14 @@
 // gather primorial-ap/ap_gpu.py:204-313), re-indexed so that one table per
 // prime serves every lane of every wheel.
 //
-// S2 (compaction rounds).  S1 survivors go to a per-CTA shared-memory
-// queue (block-wide ballot/prefix compaction).  When it fills, the CTA
-// drains it through rounds over the remaining primes: every live candidate
-// is tested against a round's primes (Barrett residue plus the engine's
-// kill test), then survivors are compacted so the next round starts with
-// every lane busy -- the reference's stage 1b / stage 2 rounds
+// S2 (compaction rounds).  S1 survivors go to a per-WARP shared-memory
+// queue (ballot/prefix compaction inside the warp, so the word loop has no
+// block-wide barrier).  When it fills, the warp drains it through rounds
+// over the remaining primes: every live candidate is tested against a
+// round's primes (Barrett residue plus the engine's kill test), then the
+// survivors are compacted with ballots so the next round starts with every
+// lane busy; a short queue instead goes one candidate per warp, the lanes
+// splitting the primes -- the reference's stage 1b / stage 2 rounds
 // (euler-prime-runs/euler_gpu.py:523-709, dickson-ladders/ladder_gpu.py:
 // 349-407) without a host-visible queue.  Final survivors are appended to
 // a global candidate list with warp-aggregated atomics.
@@ -107,6 +109,24 @@ struct Pat {
     rho[I] = min(a, a - q);  // unsigned: a - q wraps when a < q
     Pat<P0, I + 1, NS>::word(spat, rho, acc);
   }
+  // Two consecutive words of the chain, each OR-ed into two accumulators
+  // by prime parity, so the loads and ORs of one prime do not wait on
+  // the previous prime's.
+  static __device__ __forceinline__ void word2(const u64* __restrict__ spat,
+                                               u32* rho, u64* acc) {
+    constexpr u32 q = fk_nth_prime(P0 + I);
+    constexpr u32 off = fk_pat_prefix(P0, I);
+    constexpr u32 st = 64u % q;
+    const u32 r0 = rho[I];
+    u32 r1 = r0 + st;
+    r1 = min(r1, r1 - q);
+    u32 r2 = r1 + st;
+    r2 = min(r2, r2 - q);
+    acc[I & 1] |= spat[off + r0];
+    acc[2 + (I & 1)] |= spat[off + r1];
+    rho[I] = r2;
+    Pat<P0, I + 1, NS>::word2(spat, rho, acc);
+  }
   static __device__ __forceinline__ void setup(u32* rho, u64 R, u64 u0,
                                                const u32* __restrict__ xq,
                                                const u32* s_minv) {
@@ -120,6 +140,7 @@ struct Pat {
 template <int P0, int NS>
 struct Pat<P0, NS, NS> {
   static __device__ __forceinline__ void word(const u64*, u32*, u64&) {}
+  static __device__ __forceinline__ void word2(const u64*, u32*, u64*) {}
   static __device__ __forceinline__ void setup(u32*, u64, u64, const u32*,
                                                const u32*) {}
 };
@@ -138,7 +159,13 @@ struct SieveArgs {
   u64 cand_cap;
   DevCounters* ctr;
   unsigned long long* task_ctr;
+  u32 warp_queue;     // compaction: warp queues below this go one
+                      // candidate per warp
+  u32 seg_per_task;   // marking: segments per task
 };
+
+// Per-warp candidate queues: kQcap / 8 entries per warp, two buffers.
+constexpr u32 kWq = kQcap / (kBlock / 32);
 
 struct SieveSmem {
   u32 qa[kQcap];
@@ -161,31 +188,47 @@ __host__ __device__ constexpr u32 pat_bytes() {
   return ((fk_pat_prefix(P0, kNS) + 1) / 2) * 16;  // padded to 16 bytes
 }
 
-// Drain the queue: rounds over the per-candidate primes, then append the
-// survivors to the global candidate list.
+// A queued candidate: the chain (thread of the CTA), the word within the
+// chain and the bit within the word.
+__device__ __forceinline__ u64 cand_value(const SieveSmem& S, u32 code,
+                                          u64 M) {
+  const u32 t = code >> 22;
+  const u64 u = 64ull * (S.chain_w0[t] + ((code >> 6) & 0xFFFFu)) +
+                (code & 63u);
+  return u * M + S.chain_R[t];
+}
+
+__device__ __forceinline__ void emit_cand(const SieveArgs& a, u64 v,
+                                          u32 gitem, u64 p) {
+  if (p < a.cand_cap) {
+    a.cand_key[p] = v;
+    a.cand_item[p] = gitem;
+  } else {
+    atomicOr(&a.ctr->overflow, 1u);
+  }
+}
+
+// Drain one warp's queue (n candidates in qin; qout is the second buffer):
+// rounds over the per-candidate primes with ballot compaction, a short
+// queue one candidate per warp over every remaining prime, then the
+// survivors appended to the global list.  Warp-synchronous: every lane of
+// the warp calls it with the same n.
 template <int KIND>
-__device__ void drain(SieveSmem& S, u32 n, const DevEngine& e,
-                      const DevItem& it, u32 gitem, const SieveArgs& a,
-                      u64& ntest) {
-  u32* qin = S.qa;
-  u32* qout = S.qb;
+__device__ void warp_drain(u32* qin, u32* qout, u32 n, const SieveSmem& S,
+                           const DevEngine& e, const DevItem& it, u32 gitem,
+                           const SieveArgs& a, u32 wq_short, u64& ntest) {
+  const u32 lane = threadIdx.x & 31;
+  const u32 lt = (1u << lane) - 1u;
   const u32* __restrict__ xq = a.xq + it.xq_off;
   const u64 M = e.M;
   for (u32 r = 0; r < e.nrounds && n > 0; ++r) {
     const u32 i0 = __ldg(e.rounds + r), i1 = __ldg(e.rounds + r + 1);
-    if (n < (u32)kWarpMode) {
-      // Sparse queue: one warp per candidate over every remaining prime,
-      // the lanes splitting the primes 32 at a time and voting after each
-      // group (the reference's warp-per-candidate deep rounds,
-      // dickson-ladders/ladder_gpu.py:378-407), so a lone deep survivor
-      // no longer runs thousands of primes on one lane of an idle warp.
-      const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-      for (u32 idx = wid; idx < n; idx += kBlock / 32) {
-        const u32 code = qin[idx];
-        const u32 t = code >> 22;
-        const u64 u = 64ull * (S.chain_w0[t] + ((code >> 6) & 0xFFFFu)) +
-                      (code & 63u);
-        const u64 v = u * M + S.chain_R[t];
+    if (n < wq_short) {
+      // one candidate per warp, the lanes splitting the primes 32 at a
+      // time and voting after each group (the reference's warp-per-
+      // candidate deep rounds, dickson-ladders/ladder_gpu.py:378-407)
+      for (u32 idx = 0; idx < n; ++idx) {
+        const u64 v = cand_value(S, qin[idx], M);
         bool dead = false;
         for (u32 b = i0; b < e.NP && !dead; b += 32) {
           const u32 i = b + lane;
@@ -199,75 +242,71 @@ __device__ void drain(SieveSmem& S, u32 n, const DevEngine& e,
           }
           dead = __any_sync(0xffffffffu, kill);
         }
-        if (!dead && lane == 0) {
-          const unsigned long long p = atomicAdd(&a.ctr->ncand, 1ull);
-          if (p < a.cand_cap) {
-            a.cand_key[p] = v;
-            a.cand_item[p] = gitem;
-          } else {
-            atomicOr(&a.ctr->overflow, 1u);
-          }
-        }
+        if (!dead && lane == 0)
+          emit_cand(a, v, gitem, atomicAdd(&a.ctr->ncand, 1ull));
       }
-      __syncthreads();
+      __syncwarp();
       return;
     }
-    u32 mask = 0;
-    int k = 0;
-    for (u32 idx = threadIdx.x; idx < n; idx += kBlock, ++k) {
-      const u32 code = qin[idx];
-      const u32 t = code >> 22;
-      const u64 u = 64ull * (S.chain_w0[t] + ((code >> 6) & 0xFFFFu)) +
-                    (code & 63u);
-      const u64 v = u * M + S.chain_R[t];
-      bool alive = true;
-      u32 i = i0;
-      for (; i < i1; ++i) {
-        const PrimeRec pr = e.recs[i];
-        u32 rr = fk_bmod(v, pr.q, pr.magic) + __ldg(xq + i);
-        rr = min(rr, rr - pr.q);
-        if (kill_test<KIND>(pr, rr, e.lists, S.sbits, e.xxmax, e.n)) {
-          alive = false;
-          break;
+    u32 out = 0;
+    for (u32 base = 0; base < n; base += 32) {
+      const u32 idx = base + lane;
+      bool alive = false;
+      u32 code = 0;
+      if (idx < n) {
+        code = qin[idx];
+        const u64 v = cand_value(S, code, M);
+        alive = true;
+        u32 i = i0;
+        for (; i < i1; ++i) {
+          const PrimeRec pr = e.recs[i];
+          u32 rr = fk_bmod(v, pr.q, pr.magic) + __ldg(xq + i);
+          rr = min(rr, rr - pr.q);
+          if (kill_test<KIND>(pr, rr, e.lists, S.sbits, e.xxmax, e.n)) {
+            alive = false;
+            break;
+          }
         }
+        ntest += (i - i0) + (alive ? 0 : 1);
       }
-      ntest += (i - i0) + (alive ? 0 : 1);
-      mask |= (u32)alive << k;
+      const u32 bal = __ballot_sync(0xffffffffu, alive);
+      if (alive) qout[out + __popc(bal & lt)] = code;
+      out += __popc(bal);
     }
-    u32 tot;
-    u32 pos = block_scan(__popc(mask), S.warp, &tot);
-    k = 0;
-    for (u32 idx = threadIdx.x; idx < n; idx += kBlock, ++k)
-      if ((mask >> k) & 1u) qout[pos++] = qin[idx];
-    __syncthreads();
+    __syncwarp();
     u32* t = qin;
     qin = qout;
     qout = t;
-    n = tot;
+    n = out;
   }
-  // emit survivors
-  for (u32 idx = threadIdx.x; idx < n; idx += kBlock) {
-    const u32 code = qin[idx];
-    const u32 t = code >> 22;
-    const u64 u = 64ull * (S.chain_w0[t] + ((code >> 6) & 0xFFFFu)) +
-                  (code & 63u);
-    const u64 v = u * M + S.chain_R[t];
-    const u32 act = __activemask();
-    const int leader = __ffs(act) - 1;
-    const u32 lanemask = (1u << (threadIdx.x & 31)) - 1;
-    unsigned long long base = 0;
-    if ((int)(threadIdx.x & 31) == leader)
-      base = atomicAdd(&a.ctr->ncand, (unsigned long long)__popc(act));
-    base = __shfl_sync(act, base, leader);
-    const u64 p = base + __popc(act & lanemask);
-    if (p < a.cand_cap) {
-      a.cand_key[p] = v;
-      a.cand_item[p] = gitem;
-    } else {
-      atomicOr(&a.ctr->overflow, 1u);
-    }
+  // emit survivors: one atomic per warp
+  if (n) {
+    u64 base = 0;
+    if (lane == 0) base = atomicAdd(&a.ctr->ncand, (unsigned long long)n);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (u32 idx = lane; idx < n; idx += 32)
+      emit_cand(a, cand_value(S, qin[idx], M), gitem, base + idx);
   }
-  __syncthreads();
+  __syncwarp();
+}
+
+__device__ __forceinline__ void drain_any(u32* qin, u32* qout, u32 n,
+                                          const SieveSmem& S,
+                                          const DevEngine& e,
+                                          const DevItem& it, u32 gitem,
+                                          const SieveArgs& a, u32 wq_short,
+                                          u64& ntest) {
+  switch (e.kind) {
+    case KIND_EULER:
+      warp_drain<KIND_EULER>(qin, qout, n, S, e, it, gitem, a, wq_short, ntest);
+      break;
+    case KIND_DICKSON:
+      warp_drain<KIND_DICKSON>(qin, qout, n, S, e, it, gitem, a, wq_short, ntest);
+      break;
+    default:
+      warp_drain<KIND_AP>(qin, qout, n, S, e, it, gitem, a, wq_short, ntest);
+      break;
+  }
 }
 
 template <int P0>
@@ -362,73 +401,81 @@ __global__ void __launch_bounds__(kBlock, 2) k_sieve(SieveArgs a) {
     u32 rho[kNS];
     Pat<P0, 0, kNS>::setup(rho, R, 64ull * w0, a.xq + it.xq_off, S.minv);
     const u64 U = it.U;
+    const u32 wl = tid & 31, wid = tid >> 5;
+    u32* wq = S.qa + wid * kWq;
+    u32* wq2 = S.qb + wid * kWq;
+    const u32 wq_short = a.warp_queue;
     u32 qn = 0;
     u64 ntest = 0, nword = 0;
-    __syncthreads();
-    for (u32 wi = 0; wi < it.Tc; ++wi) {
-      const u64 w = w0 + wi;
-      u64 surv = 0;
-      if (active && 64ull * w < U) {
-        ++nword;
-        u64 acc = 0;
-        Pat<P0, 0, kNS>::word(spat, rho, acc);
-        const u64 left = U - 64ull * w;
-        u64 valid = left >= 64 ? ~0ull : ((1ull << left) - 1ull);
-        if (w == 0 && R < it.lo_off) valid &= ~1ull;
-        if (left <= 64 && R >= it.hi_last) valid &= ~(1ull << (left - 1));
-        surv = ~acc & valid;
+    __syncwarp();
+    for (u32 wi = 0; wi < it.Tc; wi += 2) {
+      // two words of the chain: w0 + wi and w0 + wi + 1
+      u64 sv[2] = {0, 0};
+      if (active) {
+        u64 acc[4] = {0, 0, 0, 0};
+        Pat<P0, 0, kNS>::word2(spat, rho, acc);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const u64 w = w0 + wi + k;
+          if (wi + k >= it.Tc || 64ull * w >= U) continue;
+          ++nword;
+          const u64 left = U - 64ull * w;
+          u64 valid = left >= 64 ? ~0ull : ((1ull << left) - 1ull);
+          if (w == 0 && R < it.lo_off) valid &= ~1ull;
+          if (left <= 64 && R >= it.hi_last) valid &= ~(1ull << (left - 1));
+          sv[k] = ~(acc[k * 2] | acc[k * 2 + 1]) & valid;
+        }
       }
-      // push this word's survivors; drain first when they do not fit, and
-      // when one word-step alone overfills the queue, push the prefix that
-      // fits and drain again (every pass pushes or drains, so it ends)
+      // push the survivors into the warp's queue; drain first when they
+      // do not fit, and when one step alone overfills an empty queue push
+      // the prefix that fits and drain again (every pass pushes or drains,
+      // so it ends)
       for (;;) {
-        const u32 c = __popcll(surv);
-        u32 tot;
-        u32 pos = block_scan(c, S.warp, &tot);
+        const u32 c = __popcll(sv[0]) + __popcll(sv[1]);
+        const u32 tot = __reduce_add_sync(0xffffffffu, c);
         if (tot == 0) break;
-        if (qn + tot <= (u32)kQcap) {
-          pos += qn;
-          while (surv) {
-            const int b = __ffsll((long long)surv) - 1;
-            surv &= surv - 1;
-            S.qa[pos++] = ((u32)tid << 22) | (wi << 6) | (u32)b;
+        if (qn + tot > kWq && qn > 0) {
+          drain_any(wq, wq2, qn, S, e, it, gitem, a, wq_short, ntest);
+          qn = 0;
+          continue;
+        }
+        // exclusive prefix of c over the warp
+        u32 x = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const u32 y = __shfl_up_sync(0xffffffffu, x, o);
+          if (wl >= (u32)o) x += y;
+        }
+        u32 pos = qn + x - c;
+        const u32 end = min(qn + tot, (u32)kWq);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          while (sv[k] && pos < end) {
+            const int b = __ffsll((long long)sv[k]) - 1;
+            sv[k] &= sv[k] - 1;
+            wq[pos++] = ((u32)tid << 22) | ((wi + k) << 6) | (u32)b;
           }
+        }
+        __syncwarp();
+        if (qn + tot <= (u32)kWq) {
           qn += tot;
           break;
         }
-        if (qn == 0) {
-          u32 room = pos < (u32)kQcap ? min(c, (u32)kQcap - pos) : 0u;
-          while (room--) {
-            const int b = __ffsll((long long)surv) - 1;
-            surv &= surv - 1;
-            S.qa[pos++] = ((u32)tid << 22) | (wi << 6) | (u32)b;
-          }
-          qn = kQcap;
-        }
-        __syncthreads();
-        switch (e.kind) {
-          case KIND_EULER: drain<KIND_EULER>(S, qn, e, it, gitem, a, ntest); break;
-          case KIND_DICKSON: drain<KIND_DICKSON>(S, qn, e, it, gitem, a, ntest); break;
-          default: drain<KIND_AP>(S, qn, e, it, gitem, a, ntest); break;
-        }
+        drain_any(wq, wq2, kWq, S, e, it, gitem, a, wq_short, ntest);
         qn = 0;
       }
-      __syncthreads();
     }
-    switch (e.kind) {
-      case KIND_EULER: drain<KIND_EULER>(S, qn, e, it, gitem, a, ntest); break;
-      case KIND_DICKSON: drain<KIND_DICKSON>(S, qn, e, it, gitem, a, ntest); break;
-      default: drain<KIND_AP>(S, qn, e, it, gitem, a, ntest); break;
-    }
+    drain_any(wq, wq2, qn, S, e, it, gitem, a, wq_short, ntest);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       ntest += __shfl_down_sync(0xffffffffu, ntest, o);
       nword += __shfl_down_sync(0xffffffffu, nword, o);
     }
-    if ((tid & 31) == 0) {
+    if (wl == 0) {
       if (ntest) atomicAdd(&a.ctr->s2_tests, (unsigned long long)ntest);
       if (nword) atomicAdd(&a.ctr->s1_words, (unsigned long long)nword);
     }
+    __syncthreads();
   }
 }
 

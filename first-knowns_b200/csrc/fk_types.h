@@ -27,7 +27,8 @@ constexpr int kMaxRounds = 64;
 constexpr int kSortSmem = 4096;   // entries a CTA sorts in shared memory
 constexpr int kClassChunk = 128;  // candidates a warp fetches at once
 constexpr int kBucketFill = 1024; // expected entries per ordering bucket
-constexpr int kWarpMode = 512;    // queue below which rounds go warp-wide
+constexpr int kWarpMode = 32;     // warp queue below which a candidate
+                                  // takes a whole warp
 constexpr int kSeg = 32768;       // marking: periods per shared segment
 constexpr int kSegPerTask = 8;    // marking: segments per task
 constexpr int kMarkPrimes = 6528; // marking: most primes one engine marks

@@ -80,16 +80,24 @@ class GpuEngine:
         for q in self.wheel_primes:
             M *= q
         self.M = M
-        # the device line: 23# when its lane table fits, else 13#
+        # the device lines: the widest wheel whose lane table stays within
+        # 2^26 entries (31#, else 23#), 23# for mid-length windows, 13#
+        # for short ones
         self._p0_wide = 9 if self.n >= 3 else 6
+        if wheel_offset_count(self.n, WHEEL_PRIMES_31) <= 1 << 26:
+            self._p0_wide = 11
         self._wide = _device_engine(self.n, self._p0_wide)
+        self._mid = (_device_engine(self.n, 9) if self._p0_wide == 11
+                     else None)
         self._narrow = _device_engine(self.n, 6)
 
     def _eng_for(self, lo, hi):
         # a window shorter than a few wide-wheel words wastes most lanes
-        if hi - lo < 64 * 4 * self._wide.M:
-            return self._narrow
-        return self._wide
+        if hi - lo >= 64 * 4 * self._wide.M:
+            return self._wide
+        if self._mid is not None and hi - lo >= 64 * 4 * self._mid.M:
+            return self._mid
+        return self._narrow
 
     def _check(self, lo, hi):
         lo, hi = int(lo), int(hi)

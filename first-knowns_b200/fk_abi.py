@@ -58,10 +58,24 @@ class Stats(ctypes.Structure):
                 ("imad_alg", _u64), ("sprp_values", _u64),
                 ("marks", _u64), ("h2d_bytes", _u64), ("d2h_bytes", _u64),
                 ("sieve_ms", ctypes.c_float), ("classify_ms", ctypes.c_float),
-                ("total_ms", ctypes.c_float), ("pad", _u32)]
+                ("total_ms", ctypes.c_float), ("mark_ms", ctypes.c_float),
+                ("rounds_ms", ctypes.c_float), ("pad", _u32)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_ if f != "pad"}
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("sieve_ctas_per_sm", _u32), ("mark_ctas_per_sm", _u32),
+                ("chains_per_sm", _u32), ("warp_queue", _u32),
+                ("seg_per_task", _u32), ("classify_ctas_per_sm", _u32),
+                ("mark_limit", _u32), ("mark_bias", ctypes.c_float)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+TUNING_FIELDS = [f for f, _ in Tuning._fields_]
 
 
 class BatchResult(ctypes.Structure):
@@ -113,6 +127,12 @@ SIGNATURES = {
                                         ctypes.POINTER(Stats)]),
     "fk_engine_stats": (ctypes.c_int32, [ctypes.c_void_p,
                                          ctypes.POINTER(Stats)]),
+    "fk_batch_set_tuning": (ctypes.c_int32, [ctypes.c_void_p,
+                                             ctypes.POINTER(Tuning)]),
+    "fk_batch_get_tuning": (ctypes.c_int32, [ctypes.c_void_p,
+                                             ctypes.POINTER(Tuning)]),
+    "fk_engine_set_tuning": (ctypes.c_int32, [ctypes.c_void_p,
+                                              ctypes.POINTER(Tuning)]),
     "fk_set_device": (ctypes.c_int32, [ctypes.c_int]),
     "fk_peak": (ctypes.c_int32, [ctypes.c_int,
                                  ctypes.POINTER(ctypes.c_double)]),
@@ -242,6 +262,12 @@ class Engine:
         _check(self._lib.fk_engine_stats(self._h, ctypes.byref(st)))
         return st.as_dict()
 
+    def set_tuning(self, **kw):
+        """Kernel shape of this engine's plain calls (fk_tuning fields;
+        unnamed fields keep their values)."""
+        _check(self._lib.fk_engine_set_tuning(self._h,
+                                              ctypes.byref(_tuning(kw))))
+
     def depths(self, xs, cap):
         """Chain depth of each explicit chain start in xs."""
         xs = [int(x) for x in xs]
@@ -340,11 +366,30 @@ class Batch:
         _check(self._lib.fk_batch_stats(self._h, ctypes.byref(st)))
         return st.as_dict()
 
+    def get_tuning(self):
+        t = Tuning()
+        _check(self._lib.fk_batch_get_tuning(self._h, ctypes.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        """Set fk_tuning fields by name; unnamed fields keep their values."""
+        _check(self._lib.fk_batch_set_tuning(self._h,
+                                             ctypes.byref(_tuning(kw))))
+
     def last_ms(self):
         a, c, t = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
         _check(self._lib.fk_batch_last_ms(self._h, ctypes.byref(a),
                                           ctypes.byref(c), ctypes.byref(t)))
         return float(a.value), float(c.value), float(t.value)
+
+
+def _tuning(kw):
+    t = Tuning()
+    for k, v in kw.items():
+        if k not in TUNING_FIELDS:
+            raise ValueError(f"unknown tuning field {k}")
+        setattr(t, k, float(v) if k == "mark_bias" else int(v))
+    return t
 
 
 def sprp(values, base2_only=False):
@@ -380,9 +425,10 @@ def set_device(device):
 
 def peak(which):
     """Measured peak: 'imad' -> 32-bit multiply-adds/s, 'smem' -> shared
-    load bytes/s."""
+    load bytes/s, 'smem_st' -> shared byte stores/s."""
     out = ctypes.c_double()
-    _check(load().fk_peak({"imad": 0, "smem": 1}[which], ctypes.byref(out)))
+    _check(load().fk_peak({"imad": 0, "smem": 1, "smem_st": 2}[which],
+                          ctypes.byref(out)))
     return float(out.value)
 
 

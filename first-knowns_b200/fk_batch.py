@@ -101,6 +101,8 @@ class BatchEngine:
                 self._batch.close()
             self._batch = fk_abi.Batch(self.engset.engines())
             self._nengines = n
+            if getattr(self, "_tuning", None):
+                self._batch.set_tuning(**self._tuning)
         return self._batch
 
     def run_arrays(self, intervals, graph=True):
@@ -149,6 +151,15 @@ class BatchEngine:
         """Device work counters and event times of the last run."""
         return self._batch.stats()
 
+    def tuning(self):
+        """The batch's kernel shape (fk_tuning fields)."""
+        return self._ensure().get_tuning()
+
+    def set_tuning(self, **kw):
+        """Set fk_tuning fields (the autotuner's knobs) by name."""
+        self._tuning = dict(getattr(self, "_tuning", {}), **kw)
+        self._ensure().set_tuning(**kw)
+
 
 class PlainEngine:
     """The same intervals, one fk_hunt call each."""
@@ -156,11 +167,27 @@ class PlainEngine:
     def __init__(self, engset=None):
         self.engset = engset or EngineSet()
 
+    def set_tuning(self, **kw):
+        """Apply fk_tuning fields to every engine's plain calls, and to
+        engines created later."""
+        self._tuning = dict(getattr(self, "_tuning", {}), **kw)
+        self._tuned = set()
+        for e in self.engset.engines():
+            e.set_tuning(**self._tuning)
+            self._tuned.add(id(e))
+
+    def _engine(self, iv):
+        e = self.engset.get(self.engset.key_for(iv))
+        if getattr(self, "_tuning", None) and id(e) not in self._tuned:
+            e.set_tuning(**self._tuning)
+            self._tuned.add(id(e))
+        return e
+
     def run_arrays(self, intervals):
         """Per interval (offsets, depths) as BatchEngine.run_arrays."""
         out = []
         for iv in intervals:
-            e = self.engset.get(self.engset.key_for(iv))
+            e = self._engine(iv)
             lo, hi = line_range(iv, e.W if iv.kind == DICKSON else 1)
             out.append(e.hunt(lo, hi, iv.threshold, iv.cap))
         return out
@@ -168,7 +195,7 @@ class PlainEngine:
     def run(self, intervals):
         out = []
         for iv in intervals:
-            e = self.engset.get(self.engset.key_for(iv))
+            e = self._engine(iv)
             W = e.W if iv.kind == DICKSON else 1
             lo, hi = line_range(iv, W)
             off, dep = e.hunt(lo, hi, iv.threshold, iv.cap)

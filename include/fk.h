@@ -46,7 +46,7 @@ typedef struct fk_params {
   uint32_t kind;      /* FK_EULER / FK_DICKSON / FK_AP                       */
   uint32_t n;         /* filter: values x^2+x+p for x < n; m = 1..n; AP n     */
   uint32_t q2;        /* sieve depth: primes below q2 (0: 65536)              */
-  uint32_t p0;        /* first pattern-sieve prime index: 6, 7, 9 or 12       *
+  uint32_t p0;        /* first pattern-sieve prime index: 6, 7, 9 or 11       *
                        * (all sieve primes below it are folded into the       *
                        * wheel); 0 picks a default for the kind               */
   uint64_t d_lo, d_hi;/* AP difference (0, 0: the n-th primorial)             */
@@ -149,6 +149,32 @@ fk_status fk_batch_ready(fk_batch* b, int* ready);
 fk_status fk_batch_last_ms(const fk_batch* b, float* sieve_ms,
                            float* classify_ms, float* total_ms);
 
+/* Kernel shape of a batch (or of an engine's plain calls).  None of these
+ * changes a result; they only move time.  fk_tune.py searches them.
+ * Zero in any field keeps that field's current value.                   */
+typedef struct fk_tuning {
+  uint32_t sieve_ctas_per_sm;    /* k_sieve persistent grid: CTAs per SM (1-2)  */
+  uint32_t mark_ctas_per_sm;     /* k_mark persistent grid: CTAs per SM (1-3)   */
+  uint32_t chains_per_sm;        /* lanes are cut into chains until about this *
+                                  * many chains per SM exist (64-65536)        */
+  uint32_t warp_queue;           /* compaction: a warp's queue shorter than    *
+                                  * this runs one candidate per warp over all  *
+                                  * later primes (1-512)                       */
+  uint32_t seg_per_task;         /* marking: 32768-period segments per task    *
+                                  * (1-64)                                     */
+  uint32_t classify_ctas_per_sm; /* k_classify grid: CTAs per SM (1-32)        */
+  uint32_t mark_limit;           /* sieve-prime bound of the marking sieve:    *
+                                  * primes below it are marked, the rest are   *
+                                  * tested per candidate (2^16 = all marked)   */
+  float mark_bias;               /* an item is marked when the modelled cost   *
+                                  * of marking is below mark_bias times that   *
+                                  * of the compaction rounds                   */
+} fk_tuning;
+fk_status fk_batch_set_tuning(fk_batch* b, const fk_tuning* t);
+fk_status fk_batch_get_tuning(const fk_batch* b, fk_tuning* out);
+/* The same for the engine's plain calls (fk_sieve / fk_hunt / fk_dense). */
+fk_status fk_engine_set_tuning(fk_engine* e, const fk_tuning* t);
+
 /* Counters of the last run (device-side work accounting). */
 typedef struct fk_stats {
   uint64_t launches;     /* kernels launched by the run                      */
@@ -165,6 +191,8 @@ typedef struct fk_stats {
   uint64_t h2d_bytes;    /* host-to-device bytes the run copied             */
   uint64_t d2h_bytes;    /* device-to-host bytes the run copied             */
   float sieve_ms, classify_ms, total_ms;
+  float mark_ms;         /* device time of the marking-sieve launches       */
+  float rounds_ms;       /* device time of the pattern + rounds launches    */
   uint32_t pad;
 } fk_stats;
 fk_status fk_batch_stats(const fk_batch* b, fk_stats* out);
@@ -206,7 +234,8 @@ const char* fk_version(void);
 fk_status fk_set_device(int device);
 /* Measured device peaks for the rooflines: which = 0 gives 32-bit integer
  * multiply-adds per second (IMAD, lo and hi halves alternating), which = 1
- * shared-memory load bytes per second (64-bit, bank-conflict free). */
+ * shared-memory load bytes per second (64-bit, bank-conflict free),
+ * which = 2 shared-memory byte stores per second (bank-conflict free). */
 fk_status fk_peak(int which, double* per_second);
 
 #ifdef __cplusplus

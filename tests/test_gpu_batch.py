@@ -109,3 +109,49 @@ def test_submit_ready_wait():
     st = be.stats()
     assert st["launches"] >= 5 and st["total_ms"] > 0
     assert fk_abi.peak("imad") > 1e12
+
+
+def test_tuning_changes_no_result():
+    """Every fk_tuning knob only moves time: the batch stream is identical
+    under each setting, and the plain engine agrees under another one."""
+    from fk_batch import BatchEngine, PlainEngine
+    ivs = _clipped(200, 81, clip=1 << 30)
+    be = BatchEngine(ivs)
+    ref = be.run_arrays(ivs, graph=False)
+    assert sum(x[0].size for x in ref) > 50
+    settings = [dict(mark_limit=8192), dict(mark_limit=2048, mark_bias=2.0),
+                dict(seg_per_task=1, mark_bias=4.0),
+                dict(warp_queue=4, chains_per_sm=512),
+                dict(warp_queue=512, mark_bias=0.25),
+                dict(sieve_ctas_per_sm=1, mark_ctas_per_sm=1,
+                     classify_ctas_per_sm=2),
+                dict(sieve_ctas_per_sm=2, mark_ctas_per_sm=3,
+                     classify_ctas_per_sm=8, mark_limit=65536,
+                     seg_per_task=8, warp_queue=32, mark_bias=1.0,
+                     chains_per_sm=2048)]
+    for kw in settings:
+        be.set_tuning(**kw)
+        assert _same(be.run_arrays(ivs, graph=True), ref), kw
+    pe = PlainEngine(be.engset)
+    pe.set_tuning(mark_limit=16384, seg_per_task=3)
+    assert _same(pe.run_arrays(ivs), ref)
+    with pytest.raises(ValueError):
+        be.set_tuning(mark_ctas_per_sm=9)
+
+
+def test_wide_wheel_intervals_match_the_narrow_wheel():
+    """Long intervals run on the 17# wheel; the streams equal those of the
+    13# wheel on the same intervals, in a mix with short ones."""
+    import fk_workloads as W
+    from fk_batch import BatchEngine, EngineSet
+    long_ivs = [W.Interval(k, n, lo, lo + (1 << 35), n, W.default_cap(k, n))
+                for k, n, lo in ((W.EULER, 5, 10 ** 15),
+                                 (W.DICKSON, 6, 10 ** 13),
+                                 (W.AP, 7, 3 * 10 ** 16))]
+    ivs = long_ivs + _clipped(40, 82)
+    wide = BatchEngine(ivs)
+    assert all(wide.engset.key_for(iv)[-1] == 7 for iv in long_ivs)
+    narrow = BatchEngine(ivs, engset=EngineSet(wide=False))
+    a = wide.run_arrays(ivs)
+    assert _same(a, narrow.run_arrays(ivs))
+    assert sum(x[0].size for x in a[:3]) > 100
