@@ -61,6 +61,15 @@ __host__ __device__ constexpr u32 fk_nth_prime(int i) {
   return c;
 }
 
+// 64^-1 mod q for an odd prime q, at compile time: the pattern tables are
+// stored in the order of 64-period steps, so a word's table index is its
+// phase times this inverse.
+__host__ __device__ constexpr u32 fk_inv64(u32 q) {
+  u32 x = 1;
+  while ((64u * x) % q != 1u) ++x;
+  return x;
+}
+
 // Word offset of pattern prime I (counted from prime index P0) in the
 // concatenated pattern table: the sum of the I primes before it.
 __host__ __device__ constexpr u32 fk_pat_prefix(int P0, int I) {

@@ -330,18 +330,24 @@ static fk_status build_engine(fk_engine* e) {
   }
   const u32 NP = (u32)e->sieve.size();
   // ---- pattern tables (the first kNS sieve primes) -----------------------
+  // entry k of prime q's table is the mask of the 64 periods from phase
+  // rho = 64k mod q, so a lane's consecutive words are consecutive entries
+  // and the 32 lanes of a warp sweeping one lane read 32 consecutive
+  // entries (no bank conflict)
   std::vector<u64> pat;
-  std::vector<u32> minv(kNS);
+  std::vector<u32> minv(kNS), i64(kNS);
   for (int i = 0; i < kNS; ++i) {
     const u32 q = e->sieve[i];
     if (q != fk_nth_prime((int)P0 + i))
       return set_err(FK_ERR_DEVICE, "pattern prime layout mismatch");
     const u64 mq = e->M % q;
     const u64 mi = invmod(mq, q);
-    minv[i] = (u32)mi;
+    i64[i] = fk_inv64(q);
+    minv[i] = (u32)mulmod64(mi, i64[i], q);
     std::vector<uint8_t> g(q, 0);
     for (u32 f : e->forb[i]) g[mulmod64(f, mi, q)] = 1;
-    for (u32 rho = 0; rho < q; ++rho) {
+    for (u32 k = 0; k < q; ++k) {
+      const u32 rho = (u32)((64ull * k) % q);
       u64 w = 0;
       for (u32 b = 0; b < 64; ++b)
         if (g[(rho + b) % q]) w |= 1ull << b;
@@ -470,6 +476,7 @@ static fk_status build_engine(fk_engine* e) {
   if ((st = upload(e, e->lanes, &d.lanes))) return st;
   if ((st = upload(e, pat, &d.pat, pat_bytes_for(P0)))) return st;
   if ((st = upload(e, minv, &d.pat_minv))) return st;
+  if ((st = upload(e, i64, &d.pat_i64))) return st;
   if ((st = upload(e, recs, &d.recs))) return st;
   if ((st = upload(e, c64, &d.c64))) return st;
   if ((st = upload(e, lists, &d.lists))) return st;
@@ -594,7 +601,8 @@ struct fk_batch {
 };
 
 static const fk_tuning kDefaultTuning = {2, 3, 2048, (u32)kWarpMode,
-                                         (u32)kSegPerTask, 8, 65536, 1.0f};
+                                         (u32)kSegPerTask, 8, 65536, 1.0f,
+                                         256};
 
 // Upload this batch's copy of every engine descriptor with the marked
 // prime range cut at tune.mark_limit, and the matching cost models.
@@ -784,9 +792,20 @@ static fk_status expand(fk_batch* b, const fk_item* items, u64 nitems) {
         u64 tc = (words * L + target_chains - 1) / target_chains;
         tc = std::min<u64>(std::max<u64>(tc, 1), 256);
         di.Tc = (u32)tc;
-        di.nchunk = (words + tc - 1) / tc;
-        const u64 chains = di.nchunk * L;
-        di.ntask = (chains + kBlock - 1) / kBlock;
+        // long lanes: a warp per lane, its threads on interleaved words, so
+        // a warp's pattern loads are 32 consecutive table entries
+        di.warp_lanes = words >= (u64)b->tune.warp_lane_words;
+        if (di.warp_lanes) {
+          tc = std::min<u64>(tc, (words + 31) / 32);
+          di.Tc = (u32)tc;
+          di.nchunk = (words + 32 * tc - 1) / (32 * tc);
+          const u64 chains = di.nchunk * L;    // one per warp
+          di.ntask = (chains + kBlock / 32 - 1) / (kBlock / 32);
+        } else {
+          di.nchunk = (words + tc - 1) / tc;
+          const u64 chains = di.nchunk * L;
+          di.ntask = (chains + kBlock - 1) / kBlock;
+        }
       }
       Family& f = b->fam[fam_of(e->P0, mark)];
       di.task0 = f.prefix.back();
@@ -1320,10 +1339,12 @@ fk_status fk_batch_set_tuning(fk_batch* b, const fk_tuning* t) {
   if (t->classify_ctas_per_sm) n.classify_ctas_per_sm = t->classify_ctas_per_sm;
   if (t->mark_limit) n.mark_limit = t->mark_limit;
   if (t->mark_bias > 0.0f) n.mark_bias = t->mark_bias;
+  if (t->warp_lane_words) n.warp_lane_words = t->warp_lane_words;
   if (n.sieve_ctas_per_sm > 2 || n.mark_ctas_per_sm > 3 ||
       n.chains_per_sm < 64 || n.chains_per_sm > 65536 ||
-      n.warp_queue > (u32)kWq || n.seg_per_task > 64 ||
+      n.warp_queue > (u32)kWq + 1 || n.seg_per_task > 64 ||
       n.classify_ctas_per_sm > 32 || n.mark_limit > 65536 ||
+      n.warp_lane_words < 32 ||
       !(n.mark_bias < 1e6f))
     return set_err(FK_ERR_DOMAIN, "tuning value out of range");
   b->tune = n;

@@ -33,8 +33,8 @@ namespace fk {
 struct MarkSmem {
   unsigned char bytes[kSeg];
   unsigned short off16[kMarkPrimes];  // first hit offset of each marked prime
-  u32 ph[kNS];                        // pattern phase at the segment start
-  u32 lsh[kNS];                       // the lane's shift per pattern prime
+  u32 ph[kNS];                        // table index at the segment start
+  u32 lsh[kNS];                       // the lane's index shift per prime
   u32 warp[kBlock / 32];
   u32 minv[kNS];
   u32 sbits[512];
@@ -46,26 +46,24 @@ struct MarkSmem {
   unsigned long long mbar;
 };
 
-// The two pattern words of thread t in a segment (periods 128t and
-// 128t + 64 from the segment start), from the segment's phases in shared
-// memory: each prime's table index is rebuilt on the fly with a
-// compile-time modulus, so no per-prime phase occupies a register while
-// the segment is marked.
+// The two pattern words of thread t in a segment (words 2t and 2t + 1),
+// from each prime's table index at the segment start in shared memory
+// (ph[I]; consecutive words are consecutive entries): no per-prime index
+// occupies a register while the segment is marked.
 template <int P0, int I, int NS>
 struct PatSeg {
   static __device__ __forceinline__ void words(const u64* __restrict__ spat,
-                                               const u32* ph, u32 t128,
+                                               const u32* ph, u32 t2,
                                                u64& acc0, u64& acc1) {
     constexpr u32 q = fk_nth_prime(P0 + I);
     constexpr u32 off = fk_pat_prefix(P0, I);
-    constexpr u32 st = 64u % q;
-    u32 r = ph[I] + t128 % q;
+    u32 r = ph[I] + t2 % q;
     r = min(r, r - q);
     acc0 |= spat[off + r];
-    u32 r2 = r + st;
+    u32 r2 = r + 1;
     r2 = min(r2, r2 - q);
     acc1 |= spat[off + r2];
-    PatSeg<P0, I + 1, NS>::words(spat, ph, t128, acc0, acc1);
+    PatSeg<P0, I + 1, NS>::words(spat, ph, t2, acc0, acc1);
   }
 };
 template <int P0, int NS>
@@ -186,14 +184,16 @@ __global__ void __launch_bounds__(kBlock, 3) k_mark(SieveArgs a) {
     const u64 u_start = chunk * (u64)kSeg * a.seg_per_task;
     const u64 u_end = min((u64)it.U, u_start + (u64)kSeg * a.seg_per_task);
     const u32 npm = e.NPm - e.NS;   // marked primes (the batch's bound)
-    // the lane's shift and first-segment phase for every pattern prime
+    // the lane's index shift and first-segment table index for every
+    // pattern prime: ((u + s_l) * 64^-1) mod q, s_l carrying 64^-1 already
     if (tid < kNS) {
       const PrimeRec pr = e.recs[tid];
       u32 x = xq[tid] + fk_bmod(R, pr.q, pr.magic);
       x = min(x, x - pr.q);
       const u32 sh = fk_mulmod(x, S.minv[tid], pr.q, pr.magic);
       S.lsh[tid] = sh;
-      u32 p = fk_bmod(u_start, pr.q, pr.magic) + sh;
+      u32 p = fk_mulmod(fk_bmod(u_start, pr.q, pr.magic),
+                        __ldg(e.pat_i64 + tid), pr.q, pr.magic) + sh;
       S.ph[tid] = min(p, p - pr.q);
     }
     // the first hit offset of every marked prime in the first segment
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_mark(SieveArgs a) {
       const u32 seg_len = (u32)min((u64)kSeg, u_end - useg);
       // (a) the pattern words 2*tid and 2*tid + 1
       u64 acc0 = 0, acc1 = 0;
-      PatSeg<P0, 0, kNS>::words(spat, S.ph, 128u * (u32)tid, acc0, acc1);
+      PatSeg<P0, 0, kNS>::words(spat, S.ph, 2u * (u32)tid, acc0, acc1);
       nword += 2;
       // zero the byte map
       {
@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_mark(SieveArgs a) {
         }
         if (tid < kNS) {
           const PrimeRec pr = e.recs[tid];
-          const u32 p = S.ph[tid] + (u32)kSeg % pr.q;
+          const u32 p = S.ph[tid] + (u32)(kSeg / 64) % pr.q;
           S.ph[tid] = min(p, p - pr.q);
         }
       }

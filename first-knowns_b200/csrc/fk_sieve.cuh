@@ -97,49 +97,46 @@ __device__ __forceinline__ bool kill_test(const PrimeRec& pr, u32 r,
 }
 
 // ---- S1 helpers, unrolled over the compile-time pattern primes ----------
+// k[I] is the lane's current TABLE INDEX for pattern prime I (entry k =
+// phase 64k mod q), so one word forward is k + 1 and STRIDE words forward
+// is k + STRIDE (mod q).
 template <int P0, int I, int NS>
 struct Pat {
-  static __device__ __forceinline__ void word(const u64* __restrict__ spat,
-                                              u32* rho, u64& acc) {
-    constexpr u32 q = fk_nth_prime(P0 + I);
-    constexpr u32 off = fk_pat_prefix(P0, I);
-    constexpr u32 st = 64u % q;
-    acc |= spat[off + rho[I]];
-    const u32 a = rho[I] + st;
-    rho[I] = min(a, a - q);  // unsigned: a - q wraps when a < q
-    Pat<P0, I + 1, NS>::word(spat, rho, acc);
-  }
-  // Two consecutive words of the chain, each OR-ed into two accumulators
-  // by prime parity, so the loads and ORs of one prime do not wait on
-  // the previous prime's.
+  // Two words of the chain, STRIDE words apart, each OR-ed into two
+  // accumulators by prime parity, so the loads and ORs of one prime do not
+  // wait on the previous prime's; the index then moves 2 * STRIDE words.
+  template <u32 STRIDE>
   static __device__ __forceinline__ void word2(const u64* __restrict__ spat,
-                                               u32* rho, u64* acc) {
+                                               u32* k, u64* acc) {
     constexpr u32 q = fk_nth_prime(P0 + I);
     constexpr u32 off = fk_pat_prefix(P0, I);
-    constexpr u32 st = 64u % q;
-    const u32 r0 = rho[I];
+    constexpr u32 st = STRIDE % q;
+    const u32 r0 = k[I];
     u32 r1 = r0 + st;
-    r1 = min(r1, r1 - q);
+    r1 = min(r1, r1 - q);  // unsigned: r1 - q wraps when r1 < q
     u32 r2 = r1 + st;
     r2 = min(r2, r2 - q);
     acc[I & 1] |= spat[off + r0];
     acc[2 + (I & 1)] |= spat[off + r1];
-    rho[I] = r2;
-    Pat<P0, I + 1, NS>::word2(spat, rho, acc);
+    k[I] = r2;
+    Pat<P0, I + 1, NS>::template word2<STRIDE>(spat, k, acc);
   }
-  static __device__ __forceinline__ void setup(u32* rho, u64 R, u64 u0,
+  // The table index of period u0 of lane R: phase (u0 + s_l) mod q with
+  // s_l = (X0 + R) * (M mod q)^-1, times 64^-1 (s_minv already carries it).
+  static __device__ __forceinline__ void setup(u32* k, u64 R, u64 u0,
                                                const u32* __restrict__ xq,
                                                const u32* s_minv) {
     constexpr u32 q = fk_nth_prime(P0 + I);
+    constexpr u32 i64 = fk_inv64(q);
     const u32 rq = (u32)(R % q);
     const u32 s = (u32)(((xq[I] + rq) % q) * (u64)s_minv[I] % q);
-    rho[I] = (u32)((u0 % q + s) % q);
-    Pat<P0, I + 1, NS>::setup(rho, R, u0, xq, s_minv);
+    k[I] = (u32)(((u32)(u0 % q) * i64 + s) % q);
+    Pat<P0, I + 1, NS>::setup(k, R, u0, xq, s_minv);
   }
 };
 template <int P0, int NS>
 struct Pat<P0, NS, NS> {
-  static __device__ __forceinline__ void word(const u64*, u32*, u64&) {}
+  template <u32 STRIDE>
   static __device__ __forceinline__ void word2(const u64*, u32*, u64*) {}
   static __device__ __forceinline__ void setup(u32*, u64, u64, const u32*,
                                                const u32*) {}
@@ -171,7 +168,8 @@ struct SieveSmem {
   u32 qa[kQcap];
   u32 qb[kQcap];
   u64 chain_R[kBlock];
-  u64 chain_w0[kBlock];
+  u64 chain_w0[kBlock];   // the thread's first word; word j is w0 + j*stride
+  u32 stride;             // 1, or 32 when a warp sweeps one lane
   u32 warp[kBlock / 32];
   u32 minv[kNS];
   u32 sbits[512];
@@ -193,7 +191,8 @@ __host__ __device__ constexpr u32 pat_bytes() {
 __device__ __forceinline__ u64 cand_value(const SieveSmem& S, u32 code,
                                           u64 M) {
   const u32 t = code >> 22;
-  const u64 u = 64ull * (S.chain_w0[t] + ((code >> 6) & 0xFFFFu)) +
+  const u64 u = 64ull * (S.chain_w0[t] +
+                         (u64)((code >> 6) & 0xFFFFu) * S.stride) +
                 (code & 63u);
   return u * M + S.chain_R[t];
 }
@@ -389,34 +388,44 @@ __global__ void __launch_bounds__(kBlock, 2) k_sieve(SieveArgs a) {
     }
     const DevEngine e = eg;
     // ---- this thread's chain -------------------------------------------
-    const u64 g = (task - a.task_prefix[S.item]) * kBlock + tid;
+    // thread layout: one lane per thread, Tc consecutive words; warp
+    // layout (long lanes): one lane per warp, thread t taking words
+    // t, t + 32, ... of a 32 * Tc word block
+    const bool wlay = it.warp_lanes != 0;
+    const u32 wl = tid & 31, wid = tid >> 5;
+    const u64 g = wlay ? (task - a.task_prefix[S.item]) * (kBlock / 32) + wid
+                       : (task - a.task_prefix[S.item]) * kBlock + tid;
     const u64 nchain = it.nchunk * e.L;
     const bool active = g < nchain;
     const u64 chunk = active ? g / e.L : 0;
     const u32 lane = active ? (u32)(g % e.L) : 0;
     const u64 R = active ? e.lanes[lane] : 0;
-    const u64 w0 = chunk * it.Tc;
+    const u64 w0 = wlay ? chunk * 32ull * it.Tc + wl : chunk * it.Tc;
+    const u32 stride = wlay ? 32u : 1u;
     S.chain_R[tid] = R;
     S.chain_w0[tid] = w0;
+    if (tid == 0) S.stride = stride;
     u32 rho[kNS];
     Pat<P0, 0, kNS>::setup(rho, R, 64ull * w0, a.xq + it.xq_off, S.minv);
     const u64 U = it.U;
-    const u32 wl = tid & 31, wid = tid >> 5;
     u32* wq = S.qa + wid * kWq;
     u32* wq2 = S.qb + wid * kWq;
     const u32 wq_short = a.warp_queue;
     u32 qn = 0;
     u64 ntest = 0, nword = 0;
-    __syncwarp();
+    __syncthreads();
     for (u32 wi = 0; wi < it.Tc; wi += 2) {
-      // two words of the chain: w0 + wi and w0 + wi + 1
+      // two words of the chain: j = wi and wi + 1
       u64 sv[2] = {0, 0};
       if (active) {
         u64 acc[4] = {0, 0, 0, 0};
-        Pat<P0, 0, kNS>::word2(spat, rho, acc);
+        if (wlay)
+          Pat<P0, 0, kNS>::template word2<32>(spat, rho, acc);
+        else
+          Pat<P0, 0, kNS>::template word2<1>(spat, rho, acc);
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
-          const u64 w = w0 + wi + k;
+          const u64 w = w0 + (u64)(wi + k) * stride;
           if (wi + k >= it.Tc || 64ull * w >= U) continue;
           ++nword;
           const u64 left = U - 64ull * w;

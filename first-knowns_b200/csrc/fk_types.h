@@ -44,8 +44,12 @@ struct DevEngine {
   uint64_t W;                     // Dickson: k = W * j
   uint64_t d_lo, d_hi;            // AP difference
   const uint64_t* lanes;          // [L] admissible residues mod M, ascending
-  const uint64_t* pat;            // pattern words, compile-time layout
-  const uint32_t* pat_minv;       // [NS] (M mod q)^-1 mod q
+  // pattern words, compile-time layout: prime q's table holds q words,
+  // entry k = the kill mask of the 64 periods from phase 64k mod q, so
+  // consecutive words of a lane are consecutive entries
+  const uint64_t* pat;
+  const uint32_t* pat_minv;       // [NS] (M mod q)^-1 * 64^-1 mod q
+  const uint32_t* pat_i64;        // [NS] 64^-1 mod q
   const PrimeRec* recs;           // [NP]
   const uint32_t* c64;            // [NP] 2^64 mod q
   const uint32_t* lists;          // explicit forbidden-residue lists
@@ -75,7 +79,9 @@ struct DevItem {
   uint64_t U;                     // periods (sieve) or x count (dense)
   uint64_t lo_off;                // first valid x - X0 (in period 0)
   uint64_t hi_last;               // valid iff R < hi_last in period U-1
-  uint32_t Tc, pad1;              // words per chain
+  uint32_t Tc;                    // words per chain (per thread)
+  uint32_t warp_lanes;            // 1: a warp sweeps one lane, thread t
+                                  // taking words t, t + 32, ...
   uint64_t nchunk;                // chains per lane
   uint64_t task0, ntask;          // first task, task count
   uint64_t xq_off;                // this item's base-residue table

@@ -69,7 +69,8 @@ class Tuning(ctypes.Structure):
     _fields_ = [("sieve_ctas_per_sm", _u32), ("mark_ctas_per_sm", _u32),
                 ("chains_per_sm", _u32), ("warp_queue", _u32),
                 ("seg_per_task", _u32), ("classify_ctas_per_sm", _u32),
-                ("mark_limit", _u32), ("mark_bias", ctypes.c_float)]
+                ("mark_limit", _u32), ("mark_bias", ctypes.c_float),
+                ("warp_lane_words", _u32)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -12,6 +12,10 @@ measure a warm one.  The cases keep device memory to a few hundred MB:
   sprp_euler4   8 Euler intervals (n = 4) of 2^34: the SPRP chains
                 (k_classify)
   mixed         256 intervals of the mixed workload, clipped to 2^28
+  euler_wide17  the Euler n = 17 pre-primality stream over [6.11e20,
+                +2e15) through the reference-API mirror (31# wheel, the
+                pattern sieve of the SCORE_WIDE window at a tenth of its
+                length)
 """
 
 import argparse
@@ -51,11 +55,33 @@ def case(name):
     raise SystemExit(f"unknown case {name}")
 
 
+def euler_wide(runs, warp_lane_words=0):
+    from euler_gpu import GpuEngine
+    eng = GpuEngine(17)
+    lo, span = 611 * 10 ** 18, 2 * 10 ** 15
+    if warp_lane_words:
+        eng._eng_for(lo, lo + span).set_tuning(
+            warp_lane_words=warp_lane_words)
+    for r in range(runs):
+        t0 = time.perf_counter()
+        s = eng.survivors_pre_mr(lo, lo + span)
+        dt = time.perf_counter() - t0
+        st = eng._eng_for(lo, lo + span).stats()
+        print(f"euler_wide17 run {r}: {dt * 1e3:.1f} ms wall, sieve "
+              f"{st['sieve_ms']:.1f} ms, {len(s)} survivors, s1_words "
+              f"{st['s1_words']}, s2_tests {st['s2_tests']}", flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", required=True)
     ap.add_argument("--runs", type=int, default=2)
+    ap.add_argument("--warp-lane-words", type=int, default=0,
+                    help="euler_wide17: lanes from this many words go one "
+                         "warp per lane (0: the engine default)")
     args = ap.parse_args()
+    if args.case == "euler_wide17":
+        return euler_wide(args.runs, args.warp_lane_words)
     ivs = case(args.case)
     be = BatchEngine(ivs)
     for r in range(args.runs):

@@ -4,7 +4,8 @@ The search space is fk_tuning (include/fk.h): CTAs per SM of the three
 persistent grids (pattern sieve + rounds, marking sieve, SPRP), chains per
 SM when lanes are cut into chains, the compaction cadence (a warp's queue
 shorter than ``warp_queue`` goes one candidate per warp), the marking task length in
-32768-period segments, the marking sieve's prime bound (primes below
+32768-period segments, the lane length from which a warp sweeps one lane,
+the marking sieve's prime bound (primes below
 ``mark_limit`` are marked, the rest tested per candidate) and the bias
 between marking and compaction rounds.  None of them can change a result;
 they only move time.
@@ -31,6 +32,7 @@ SPACE = {
     "sieve_ctas_per_sm": [1, 2],
     "mark_ctas_per_sm": [2, 3],
     "classify_ctas_per_sm": [4, 8, 16],
+    "warp_lane_words": [64, 1024, 1 << 30],
 }
 
 DEFAULT_PATH = pathlib.Path(__file__).resolve().parent / "tuning.json"

@@ -159,7 +159,7 @@ typedef struct fk_tuning {
                                   * many chains per SM exist (64-65536)        */
   uint32_t warp_queue;           /* compaction: a warp's queue shorter than    *
                                   * this runs one candidate per warp over all  *
-                                  * later primes (1-512)                       */
+                                  * later primes (1-513; 513: always)         */
   uint32_t seg_per_task;         /* marking: 32768-period segments per task    *
                                   * (1-64)                                     */
   uint32_t classify_ctas_per_sm; /* k_classify grid: CTAs per SM (1-32)        */
@@ -169,6 +169,8 @@ typedef struct fk_tuning {
   float mark_bias;               /* an item is marked when the modelled cost   *
                                   * of marking is below mark_bias times that   *
                                   * of the compaction rounds                   */
+  uint32_t warp_lane_words;      /* lanes of at least this many 64-period      *
+                                  * words are swept one warp per lane (>= 32)  */
 } fk_tuning;
 fk_status fk_batch_set_tuning(fk_batch* b, const fk_tuning* t);
 fk_status fk_batch_get_tuning(const fk_batch* b, fk_tuning* out);

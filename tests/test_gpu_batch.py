@@ -121,6 +121,8 @@ def test_tuning_changes_no_result():
     assert sum(x[0].size for x in ref) > 50
     settings = [dict(mark_limit=8192), dict(mark_limit=2048, mark_bias=2.0),
                 dict(seg_per_task=1, mark_bias=4.0),
+                dict(warp_lane_words=32, mark_limit=4096),
+                dict(warp_lane_words=1 << 30),
                 dict(warp_queue=4, chains_per_sm=512),
                 dict(warp_queue=512, mark_bias=0.25),
                 dict(sieve_ctas_per_sm=1, mark_ctas_per_sm=1,
@@ -128,7 +130,7 @@ def test_tuning_changes_no_result():
                 dict(sieve_ctas_per_sm=2, mark_ctas_per_sm=3,
                      classify_ctas_per_sm=8, mark_limit=65536,
                      seg_per_task=8, warp_queue=32, mark_bias=1.0,
-                     chains_per_sm=2048)]
+                     chains_per_sm=2048, warp_lane_words=256)]
     for kw in settings:
         be.set_tuning(**kw)
         assert _same(be.run_arrays(ivs, graph=True), ref), kw
