@@ -11,6 +11,8 @@ measure a warm one.  The cases keep device memory to a few hundred MB:
                 (k_sieve)
   sprp_euler4   8 Euler intervals (n = 4) of 2^34: the SPRP chains
                 (k_classify)
+  sprp_dickson6 8 Dickson intervals (n = 6) of 2^34 at k = 1e18: SPRP
+                chains on 122-bit values (four 32-bit limbs)
   mixed         256 intervals of the mixed workload, clipped to 2^28
   euler_wide17  the Euler n = 17 pre-primality stream over [6.11e20,
                 +2e15) through the reference-API mirror (31# wheel, the
@@ -42,6 +44,10 @@ def case(name):
     if name == "sprp_euler4":
         return [W.Interval(W.EULER, 4, 10 ** 16 + i * 2 ** 35,
                            10 ** 16 + i * 2 ** 35 + 2 ** 34, 4, 100)
+                for i in range(8)]
+    if name == "sprp_dickson6":
+        return [W.Interval(W.DICKSON, 6, 10 ** 18 + i * 2 ** 36,
+                           10 ** 18 + i * 2 ** 36 + 2 ** 34, 6, 14)
                 for i in range(8)]
     if name == "mixed":
         out = []
