@@ -475,7 +475,9 @@ def bench_fk(args):
     if rank == 0 and world == 1 and not args.no_serve:
         from fk_serve import ServeLoop
         reqs = W.served(count=4000, rate_hz=250.0)
-        loop = ServeLoop(eng.engset, slots=2)
+        # the server keeps its own resident tables (the served requests'
+        # engines), created before the first arrival
+        loop = ServeLoop(slots=2)
         res, lat, sst = loop.run(reqs, time_limit=args.serve_seconds)
         done = ~np.isnan(lat)
         served_c = sum(reqs[i][1].length for i in np.nonzero(done)[0])

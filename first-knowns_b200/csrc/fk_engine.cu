@@ -889,7 +889,7 @@ static fk_status enqueue(fk_batch* b, bool capturing = false) {
   FK_CUDA(cudaMemsetAsync(b->d_item_count.p, 0, (ni + 1) * sizeof(u32), s));
   FK_CUDA(cudaMemsetAsync(b->d_item_fill.p, 0, (ni + 1) * sizeof(u32), s));
   FK_CUDA(record(b->ev[0], s, capturing));
-  u64 nl = 4;  // classify, scan, bucket scatter, sort
+  u64 nl = 1;  // k_classify
   if (!b->sieve_idx.empty()) {
     ++nl;
     dim3 g(64, (u32)std::min<size_t>(b->sieve_idx.size(), 65535));
@@ -979,7 +979,7 @@ static fk_status enqueue(fk_batch* b, bool capturing = false) {
       b->d_bbase.p, b->d_nb.p, b->d_boff.p, b->d_bfill.p, b->d_sorted.p);
   k_sort_seg<<<b->nsm * 4, kBlock, 0, s>>>(b->d_sorted.p, b->d_boff.p,
                                            b->d_nbuckets.p, b->d_scratch.p);
-  nl += 6;
+  nl += 8;     // three k_scan, k_bucket_nb/_total/_count/_scatter, k_sort_seg
   FK_CUDA(cudaGetLastError());
   FK_CUDA(record(b->ev[3], s, capturing));
   FK_CUDA(cudaMemcpyAsync(b->h_ctr.p, b->d_ctr, sizeof(DevCounters),
