@@ -600,7 +600,7 @@ struct fk_batch {
   u64 h2d = 0, d2h = 0;
 };
 
-static const fk_tuning kDefaultTuning = {2, 3, 2048, (u32)kWarpMode,
+static const fk_tuning kDefaultTuning = {3, 3, 2048, (u32)kWarpMode,
                                          (u32)kSegPerTask, 8, 65536, 1.0f,
                                          256};
 
@@ -1340,7 +1340,7 @@ fk_status fk_batch_set_tuning(fk_batch* b, const fk_tuning* t) {
   if (t->mark_limit) n.mark_limit = t->mark_limit;
   if (t->mark_bias > 0.0f) n.mark_bias = t->mark_bias;
   if (t->warp_lane_words) n.warp_lane_words = t->warp_lane_words;
-  if (n.sieve_ctas_per_sm > 2 || n.mark_ctas_per_sm > 3 ||
+  if (n.sieve_ctas_per_sm > 3 || n.mark_ctas_per_sm > 3 ||
       n.chains_per_sm < 64 || n.chains_per_sm > 65536 ||
       n.warp_queue > (u32)kWq + 1 || n.seg_per_task > 64 ||
       n.classify_ctas_per_sm > 32 || n.mark_limit > 65536 ||

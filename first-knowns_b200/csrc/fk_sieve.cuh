@@ -309,7 +309,7 @@ __device__ __forceinline__ void drain_any(u32* qin, u32* qout, u32 n,
 }
 
 template <int P0>
-__global__ void __launch_bounds__(kBlock, 2) k_sieve(SieveArgs a) {
+__global__ void __launch_bounds__(kBlock, 3) k_sieve(SieveArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   u64* spat = reinterpret_cast<u64*>(smem_raw);
   SieveSmem& S = *reinterpret_cast<SieveSmem*>(smem_raw + pat_bytes<P0>());

@@ -29,7 +29,7 @@ SPACE = {
     "seg_per_task": [2, 4, 8, 16],
     "chains_per_sm": [1024, 2048, 4096, 8192],
     "warp_queue": [8, 16, 64, 128],
-    "sieve_ctas_per_sm": [1, 2],
+    "sieve_ctas_per_sm": [2, 3],
     "mark_ctas_per_sm": [2, 3],
     "classify_ctas_per_sm": [4, 8, 16],
     "warp_lane_words": [64, 1024, 1 << 30],

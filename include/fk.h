@@ -153,7 +153,7 @@ fk_status fk_batch_last_ms(const fk_batch* b, float* sieve_ms,
  * changes a result; they only move time.  fk_tune.py searches them.
  * Zero in any field keeps that field's current value.                   */
 typedef struct fk_tuning {
-  uint32_t sieve_ctas_per_sm;    /* k_sieve persistent grid: CTAs per SM (1-2)  */
+  uint32_t sieve_ctas_per_sm;    /* k_sieve persistent grid: CTAs per SM (1-3)  */
   uint32_t mark_ctas_per_sm;     /* k_mark persistent grid: CTAs per SM (1-3)   */
   uint32_t chains_per_sm;        /* lanes are cut into chains until about this *
                                   * many chains per SM exist (64-65536)        */

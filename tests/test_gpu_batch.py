@@ -127,7 +127,7 @@ def test_tuning_changes_no_result():
                 dict(warp_queue=512, mark_bias=0.25),
                 dict(sieve_ctas_per_sm=1, mark_ctas_per_sm=1,
                      classify_ctas_per_sm=2),
-                dict(sieve_ctas_per_sm=2, mark_ctas_per_sm=3,
+                dict(sieve_ctas_per_sm=3, mark_ctas_per_sm=3,
                      classify_ctas_per_sm=8, mark_limit=65536,
                      seg_per_task=8, warp_queue=32, mark_bias=1.0,
                      chains_per_sm=2048, warp_lane_words=256)]
