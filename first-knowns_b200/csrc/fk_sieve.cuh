@@ -413,6 +413,14 @@ __global__ void __launch_bounds__(kBlock, 3) k_sieve(SieveArgs a) {
     const u32 wq_short = a.warp_queue;
     u32 qn = 0;
     u64 ntest = 0, nword = 0;
+    // words below wfull end before the item's last period, so only the
+    // first word (lo_off) and the last (hi_last, U) need a validity mask
+    const u64 wfull = U ? (U - 1) >> 6 : 0;
+    if (active) {
+      // the chain's words in range: j < Tc with w0 + j*stride < ceil(U/64)
+      const u64 wend = (U + 63) >> 6;
+      if (w0 < wend) nword = min((u64)it.Tc, (wend - w0 + stride - 1) / stride);
+    }
     __syncthreads();
     for (u32 wi = 0; wi < it.Tc; wi += 2) {
       // two words of the chain: j = wi and wi + 1
@@ -426,13 +434,17 @@ __global__ void __launch_bounds__(kBlock, 3) k_sieve(SieveArgs a) {
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
           const u64 w = w0 + (u64)(wi + k) * stride;
+          const u64 s = ~(acc[k * 2] | acc[k * 2 + 1]);
+          if (w != 0 && w < wfull && wi + k < it.Tc) {
+            sv[k] = s;  // an interior word: every period is in range
+            continue;
+          }
           if (wi + k >= it.Tc || 64ull * w >= U) continue;
-          ++nword;
           const u64 left = U - 64ull * w;
           u64 valid = left >= 64 ? ~0ull : ((1ull << left) - 1ull);
           if (w == 0 && R < it.lo_off) valid &= ~1ull;
           if (left <= 64 && R >= it.hi_last) valid &= ~(1ull << (left - 1));
-          sv[k] = ~(acc[k * 2] | acc[k * 2 + 1]) & valid;
+          sv[k] = s & valid;
         }
       }
       // push the survivors into the warp's queue; drain first when they
