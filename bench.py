@@ -21,9 +21,13 @@ Reported (one JSON line, rank 0):
   plain      the plain per-interval engine on the same intervals (one
              fk_hunt call each), and batch_over_plain; bit_identical says
              both streams matched exactly
-  roofline   the dominant kernel against its measured bound (integer
-             multiply-add rate for the SPRP stage, shared-memory load rate
-             for the pattern sieve)
+  roofline   the kernel with the most device time against its measured
+             bound, and `rooflines` for all three (byte marks/s against
+             the shared byte-store rate for the marking sieve; IMADs/s
+             against the integer multiply-add rate for the rounds and the
+             SPRP stage)
+  reference_scores  the reference's own fingerprinted SCORE windows through
+             the reference-API mirrors, with its published 4090 rates
   cpu_baseline  the CPU oracle (a restatement of the reference's numpy
              engines) on a bounded sample of the workload, all host cores
   serve      p50/p99 request latency of the continuous-batching server on

@@ -2,9 +2,12 @@
 //
 // The line of one item is x = X0 + u*M + R[l]: period u in [0, U), lane l
 // over the wheel's admissible residues R mod M.  A CHAIN is one lane over
-// Tc consecutive 64-period words; one thread runs one chain, a CTA runs
-// 256 chains (a TASK), and a persistent grid pulls tasks from a device
-// counter, so thousands of items of uneven length run in one launch.
+// Tc 64-period words per thread: either one thread per lane on Tc
+// consecutive words, or -- for long lanes -- one warp per lane, thread t
+// on words t, t + 32, ... (so a warp's pattern loads are 32 consecutive
+// table entries).  A CTA runs 256 threads' chains (a TASK), and a
+// persistent grid pulls tasks from a device counter, so thousands of
+// items of uneven length run in one launch.
 //
 // S1 (pattern sieve).  For the NS pattern primes starting at prime index
 // P0 -- compile-time constants, so each prime's modulus, word step and

@@ -21,7 +21,7 @@ struct PrimeRec {
 };
 
 constexpr int kBlock = 256;       // threads per CTA, every kernel
-constexpr int kQcap = 4096;       // per-CTA candidate queue (entries)
+constexpr int kQcap = 4096;       // candidate queue entries per CTA (8 warps)
 constexpr int kNS = 32;           // pattern primes per chain
 constexpr int kMaxRounds = 64;
 constexpr int kSortSmem = 4096;   // entries a CTA sorts in shared memory

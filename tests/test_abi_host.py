@@ -110,3 +110,17 @@ def test_euler_mirror_wheel_attributes_follow_the_reference_rule():
     assert E.best_wheel(17) == E.WHEEL_PRIMES_37
     assert E.wheel_offset_count(17, E.WHEEL_PRIMES_31) == 29937600
     assert E.best_wheel(5) in (E.WHEEL_PRIMES, E.WHEEL_PRIMES_29)
+
+
+def test_generated_montgomery_header_is_current(tmp_path, monkeypatch):
+    """fk_mont32.cuh is what gen_mont32.py writes (no hand edits)."""
+    import importlib.util
+    csrc = ROOT / "first-knowns_b200" / "csrc"
+    spec = importlib.util.spec_from_file_location("gen_mont32",
+                                                  csrc / "gen_mont32.py")
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    monkeypatch.setattr(gen, "HERE", tmp_path)
+    gen.main()
+    assert (tmp_path / "fk_mont32.cuh").read_text() == \
+        (csrc / "fk_mont32.cuh").read_text()
