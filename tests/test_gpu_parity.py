@@ -151,3 +151,22 @@ def test_interval_api_matches_oracle_sweep():
     for iv, g in zip(ivs, got):
         assert g == osw.hunt_interval(iv.kind, iv.n, iv.lo, iv.hi,
                                       iv.threshold, iv.cap, iv.q2, iv.d)
+
+
+@pytest.mark.parametrize("sieve_mode,span", [("rounds", 3_400_000_000_000_000),
+                                             ("mark", 100_000_000_000_000)])
+def test_widest_family_matches_the_23_wheel(sieve_mode, span):
+    """The 31# line (p0 = 11: 37 and up as pattern primes) gives the same
+    survivor stream as the 23# line (p0 = 9), which the windows above pin
+    against the oracle; the long window's lanes are 266 words, so it runs
+    one warp per lane; unaligned ends."""
+    wide = _engine(0, 17, sieve=sieve_mode, p0=11)
+    mid = _engine(0, 17, sieve=sieve_mode, p0=9)
+    assert wide.M == 200560490130 and wide.L == 29937600
+    lo = 611 * 10 ** 18 + 12345
+    got = wide.sieve(lo, lo + span).tolist()
+    want = mid.sieve(lo, lo + span).tolist()
+    assert got == want and len(want) > 0
+    off, dep = wide.hunt(lo, lo + span, 3, 100)
+    o2, d2 = mid.hunt(lo, lo + span, 3, 100)
+    assert off.tolist() == o2.tolist() and dep.tolist() == d2.tolist()
