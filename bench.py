@@ -424,14 +424,15 @@ def bench_fk(args):
     mark_s = st_mean["mark_ms"] * 1e-3
     rnd_s = st_mean["rounds_ms"] * 1e-3
 
-    def roof(kernel, bound, work, seconds, peak, unit, scale, algo, src):
+    def roof(kernel, bound, work, seconds, peak, unit, scale, algo, src,
+             note):
         rate = work / seconds if seconds > 0 else 0.0
         return {"kernel": kernel, "bound": bound, "achieved": rate / scale,
                 "peak": peak / scale, "unit": unit,
                 "frac": rate / peak if peak else None,
                 "algorithmic": algo, "work_per_launch": work,
                 "seconds_per_launch": seconds, "traffic": None,
-                "peak_source": src}
+                "traffic_note": note, "peak_source": src}
 
     roofs = {
         "k_classify": roof(
@@ -439,14 +440,20 @@ def bench_fk(args):
             cls_s, imad_peak, "G int-multiply-adds/s", 1e9,
             "(bits-1)*(4l^2+2l) per strong-test base, l = ceil(bits/32)",
             "measured on this GPU by fk_peak (32-bit mad.lo/mad.hi "
-            "chains, 8 per thread)"),
+            "chains, 8 per thread)",
+            "candidates in, (key, depth) out: 12 B read + 16 B written per "
+            "value, about 2 GB per step at this workload; ncu of the "
+            "n = 4 Euler case: 92 MB + 7 MB for 3.1e7 values (profiles/)"),
         "k_mark": roof(
             "k_mark (marking sieve)", "smem", st["marks"], mark_s, st_peak,
             "G byte marks/s", 1e9,
             "one shared-memory byte store per (period, prime, forbidden "
             "residue) hit",
             "measured on this GPU by fk_peak (conflict-free st.shared.u8, "
-            "32 lanes)"),
+            "32 lanes)",
+            "DRAM bytes do not grow with the work (tables stay in L2 and "
+            "shared memory): ncu of the AP n = 6 case reads 0.7 MB per "
+            "launch (profiles/), so a scaled figure would be meaningless"),
         "k_sieve": roof(
             "k_sieve (pattern sieve + compaction rounds)", "imad",
             9 * st["s2_tests"], rnd_s, imad_peak, "G int-multiply-adds/s",
@@ -455,7 +462,10 @@ def bench_fk(args):
             "8, residue product: 1); the pattern stage's 32 shared loads "
             "per 64 periods ride alongside",
             "measured on this GPU by fk_peak (32-bit mad.lo/mad.hi "
-            "chains, 8 per thread)"),
+            "chains, 8 per thread)",
+            "DRAM traffic is the lane table read once (8 B per lane) plus "
+            "the candidates written; ncu of the Euler n = 17 window: "
+            "246 MB read for a 240 MB table (profiles/)"),
     }
     times = {"k_classify": cls_s, "k_mark": mark_s, "k_sieve": rnd_s}
     dominant = roofs[max(times, key=times.get)]
