@@ -37,6 +37,11 @@ Reported (one JSON line, rank 0):
 ``--impl reference`` times the reference's CPU implementation of the path
 (its numpy engines, restated in oracle/) on bounded samples of the same
 workload and prints the same line with "impl": "reference".
+
+``--profile-case NAME [--runs R]`` runs one fixed small sweep R times (the
+first is a warm-up) and prints per-run counters instead of the JSON line:
+the cases the ncu summaries under profiles/ were captured on, each a few
+hundred MB on the device (see PROFILE_CASES).
 """
 
 import argparse
@@ -82,7 +87,99 @@ def parse():
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--tune-seconds", type=float, default=60.0)
     ap.add_argument("--no-scores", action="store_true")
+    ap.add_argument("--profile-case", default=None,
+                    help="run one profiling case (PROFILE_CASES) and exit")
+    ap.add_argument("--runs", type=int, default=2,
+                    help="--profile-case: runs (the first is a warm-up)")
     return ap.parse_args()
+
+
+# ------------------------------------------------------- profiling cases ---
+
+PROFILE_CASES = {
+    "mark_ap6": "8 AP intervals (n = 6) of 2^32: the marking sieve (k_mark)",
+    "rounds_ap10": "8 AP intervals (n = 10) of 2^33: per-candidate rounds "
+                   "(k_sieve)",
+    "sprp_euler4": "8 Euler intervals (n = 4) of 2^34: the SPRP chains "
+                   "(k_classify)",
+    "sprp_dickson6": "8 Dickson intervals (n = 6) of 2^34 at k = 1e18: SPRP "
+                     "chains on 122-bit values (four 32-bit limbs)",
+    "sprp_served": "64 served-workload requests (starts 1e18-1e24) clipped "
+                   "to 2^26: SPRP on up to 165-bit values",
+    "mixed": "256 intervals of the mixed workload, clipped to 2^28 (the "
+             "bench's kernel instances: k_sieve<7>, k_mark<7>, ...)",
+    "euler_wide17": "the Euler n = 17 stream over [6.11e20, +2e15) through "
+                    "the reference-API mirror (31# wheel; the SCORE_WIDE "
+                    "window at a tenth of its length)",
+}
+
+
+def profile_intervals(name):
+    import fk_workloads as W
+    if name == "mark_ap6":
+        return [W.Interval(W.AP, 6, 10 ** 14 + i * 2 ** 33,
+                           10 ** 14 + i * 2 ** 33 + 2 ** 32 - 2 ** 32 % 30,
+                           6, 6) for i in range(8)]
+    if name == "rounds_ap10":
+        return [W.Interval(W.AP, 10, 10 ** 15 + i * 2 ** 34,
+                           10 ** 15 + i * 2 ** 34 + 2 ** 33 - 2 ** 33 % 30,
+                           10, 10) for i in range(8)]
+    if name == "sprp_euler4":
+        return [W.Interval(W.EULER, 4, 10 ** 16 + i * 2 ** 35,
+                           10 ** 16 + i * 2 ** 35 + 2 ** 34, 4, 100)
+                for i in range(8)]
+    if name == "sprp_dickson6":
+        return [W.Interval(W.DICKSON, 6, 10 ** 18 + i * 2 ** 36,
+                           10 ** 18 + i * 2 ** 36 + 2 ** 34, 6, 14)
+                for i in range(8)]
+    if name in ("mixed", "sprp_served"):
+        src = (W.mixed_batch(256) if name == "mixed" else
+               [iv for _, iv in W.served(count=64)])
+        clip = 1 << (28 if name == "mixed" else 26)
+        out = []
+        for iv in src:
+            hi = min(iv.hi, iv.lo + clip)
+            if iv.kind == W.AP:
+                hi = iv.lo + max(30, (hi - iv.lo) // 30 * 30)
+            out.append(W.Interval(iv.kind, iv.n, iv.lo, hi,
+                                  iv.threshold if name == "mixed" else 0,
+                                  iv.cap))
+        return out
+    raise SystemExit(f"unknown profile case {name}; cases: "
+                     f"{', '.join(PROFILE_CASES)}")
+
+
+def run_profile_case(name, runs):
+    if name == "euler_wide17":
+        from euler_gpu import GpuEngine
+        eng = GpuEngine(17)
+        lo, span = 611 * 10 ** 18, 2 * 10 ** 15
+        for r in range(runs):
+            t0 = time.perf_counter()
+            s = eng.survivors_pre_mr(lo, lo + span)
+            dt = time.perf_counter() - t0
+            st = eng._eng_for(lo, lo + span).stats()
+            print(f"euler_wide17 run {r}: {dt * 1e3:.1f} ms wall, sieve "
+                  f"{st['sieve_ms']:.1f} ms, {len(s)} survivors, s1_words "
+                  f"{st['s1_words']}, s2_tests {st['s2_tests']}", flush=True)
+        return 0
+    from fk_batch import BatchEngine
+    ivs = profile_intervals(name)
+    be = BatchEngine(ivs)
+    for r in range(runs):
+        t0 = time.perf_counter()
+        rows = be.run_arrays(ivs, graph=False)
+        dt = time.perf_counter() - t0
+        st = be.stats()
+        print(f"{name} run {r}: {dt * 1e3:.1f} ms wall, sieve "
+              f"{st['sieve_ms']:.1f} ms (mark {st['mark_ms']:.1f}, rounds "
+              f"{st['rounds_ms']:.1f}), classify {st['classify_ms']:.1f} ms,"
+              f" {sum(x[0].size for x in rows)} hits, {st['launches']} "
+              f"launches, candidates {st['candidates']}, s1_words "
+              f"{st['s1_words']}, s2_tests {st['s2_tests']}, marks "
+              f"{st['marks']}, sprp_values {st['sprp_values']}, imad_alg "
+              f"{st['imad_alg']}", flush=True)
+    return 0
 
 
 # ---------------------------------------------------------------- ranks ---
@@ -546,6 +643,8 @@ def bench_fk(args):
 
 def main():
     args = parse()
+    if args.profile_case:
+        return run_profile_case(args.profile_case, args.runs)
     if args.impl == "reference":
         return bench_reference(args)
     return bench_fk(args)

@@ -21,11 +21,15 @@ import functools
 
 import numpy as np
 
-from fk_abi import AP, Engine
+from fk_abi import AP, MODE_SIEVE, Batch, Engine
 
 Q2_DEFAULT = 1 << 16
 Q2_MAX = 1 << 30
 LAUNCH_U = 1 << 27
+# launches swept per device call by survivors(): each launch is one item
+# of a single batch run, so the host holds at most this many launches'
+# survivors at once
+LAUNCHES_PER_CALL = 256
 P_FLOOR = 10 ** 4
 P_CEIL = 10 ** 26
 W0 = 30
@@ -69,6 +73,7 @@ class GpuEngine:
         self.floor = max(P_FLOOR, self.q2)
         self._dev = _device_engine(self.n, self.q2, self.d)
         self._primes = None
+        self._batch = None
 
     @property
     def primes(self):
@@ -95,21 +100,26 @@ class GpuEngine:
 
     def survivors(self, base, span, launch_u=None):
         """Yield uint64 arrays of offsets o with base + o surviving,
-        ascending, one array per launch of launch_u wheel periods."""
+        ascending, one array per launch of launch_u wheel periods (empty
+        launches yield nothing), as the reference's generator does
+        (primorial-ap/ap_gpu.py:555-635).  Each launch window is one item
+        of a batch run, up to LAUNCHES_PER_CALL of them per device call, so
+        a campaign-length segment never sits on the host whole."""
         base, span = self._check(base, span)
         if span <= 0:
             return
         step = W0 * int(launch_u or self.launch_u)
-        off = self._dev.sieve(base, base + span)
-        if off.size == 0:
-            return
-        cuts = np.arange(step, span, step, dtype=np.uint64)
-        bounds = np.searchsorted(off, cuts)
-        start = 0
-        for b in list(bounds) + [off.size]:
-            if b > start:
-                yield off[start:b]
-            start = b
+        if self._batch is None:
+            self._batch = Batch([self._dev])
+        starts = list(range(0, span, step))
+        for g in range(0, len(starts), LAUNCHES_PER_CALL):
+            group = starts[g:g + LAUNCHES_PER_CALL]
+            specs = [(0, MODE_SIEVE, 0, 0, base + a, base + min(span, a + step))
+                     for a in group]
+            rows = self._batch.run(specs, graph=False)
+            for a, (off, _dep) in zip(group, rows):
+                if off.size:
+                    yield off + np.uint64(a)
 
     def hunt(self, base, span, min_depth=None):
         """[(p, depth)] for every survivor whose chain reaches min_depth."""

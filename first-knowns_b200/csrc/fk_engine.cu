@@ -140,6 +140,7 @@ struct fk_engine {
   std::vector<void*> allocs;
   u64 device_bytes = 0;
   fk_batch* plain = nullptr;  // internal single-engine batch
+  int device = 0;             // CUDA device the tables were uploaded to
   std::vector<uint64_t> res_off;
   std::vector<uint8_t> res_depth;
 };
@@ -249,8 +250,37 @@ static Cost engine_cost(const fk_engine* e, u32 NPm) {
   return c;
 }
 
+// Prime-index cuts of the compaction rounds: a round ends once the
+// modelled survival of a candidate within it falls below `cut` (or after
+// 4096 primes), so the ballot compaction between rounds runs when about
+// 1 - cut of the lanes have gone idle; at most kMaxRounds rounds.
+static constexpr double kDefaultRoundCut = 0.5;
+static std::vector<u32> compute_rounds(const fk_engine* e, double cut) {
+  const u32 NP = (u32)e->sieve.size();
+  std::vector<u32> rounds;
+  rounds.push_back(kNS);
+  double s = 1.0;
+  u32 start = kNS;
+  for (u32 i = kNS; i < NP; ++i) {
+    s *= 1.0 - (double)e->forb[i].size() / e->sieve[i];
+    if ((s < cut || i + 1 - start >= 4096) && i + 1 < NP) {
+      rounds.push_back(i + 1);
+      s = 1.0;
+      start = i + 1;
+    }
+  }
+  rounds.push_back(NP);
+  if (rounds.size() > (size_t)kMaxRounds + 1) {
+    rounds.resize(kMaxRounds);
+    rounds.push_back(NP);
+  }
+  if (NP <= (u32)kNS) rounds.assign({(u32)kNS, (u32)kNS});
+  return rounds;
+}
+
 static fk_status build_engine(fk_engine* e) {
   const fk_params& p = e->p;
+  FK_CUDA(cudaGetDevice(&e->device));
   e->kind = p.kind;
   e->n = p.n;
   e->q2 = p.q2 ? p.q2 : 65536;
@@ -393,26 +423,10 @@ static fk_status build_engine(fk_engine* e) {
     }
     recs[i] = r;
   }
-  // ---- compaction rounds: a round ends when survival within it halves ----
-  std::vector<u32> rounds;
-  rounds.push_back(kNS);
-  double s = 1.0;
-  u32 start = kNS;
-  for (u32 i = kNS; i < NP; ++i) {
-    s *= 1.0 - (double)e->forb[i].size() / e->sieve[i];
+  for (u32 i = kNS; i < NP; ++i)
     e->survival *= 1.0 - (double)e->forb[i].size() / e->sieve[i];
-    if ((s < 0.5 || i + 1 - start >= 4096) && i + 1 < NP) {
-      rounds.push_back(i + 1);
-      s = 1.0;
-      start = i + 1;
-    }
-  }
-  rounds.push_back(NP);
-  if (rounds.size() > (size_t)kMaxRounds + 1) {
-    rounds.resize(kMaxRounds);
-    rounds.push_back(NP);
-  }
-  if (NP <= (u32)kNS) rounds.assign({(u32)kNS, (u32)kNS});
+  // ---- compaction rounds: a round ends when survival within it halves ----
+  const std::vector<u32> rounds = compute_rounds(e, kDefaultRoundCut);
   // ---- marking tables: u-residue lists for every prime, (M mod q)^-1 ------
   std::vector<u32> minv_all(NP), gaux(NP), glist;
   u32 NPm = NS_marked_end(e);
@@ -577,6 +591,7 @@ struct fk_batch {
   DevBuf<u64> d_bbase, d_boff;
   DevBuf<unsigned long long> d_task_ctr;
   DevBuf<u32> d_nitems;
+  DevBuf<u32> d_rounds;         // per engine: this batch's round cuts
   DevCounters* d_ctr = nullptr;
   PinBuf<DevItem> h_items;
   PinBuf<DevCounters> h_ctr;
@@ -598,11 +613,13 @@ struct fk_batch {
   int pending_graph = 0;
   u64 last_launches = 0;
   u64 h2d = 0, d2h = 0;
+  u32 reruns = 0;               // overflow reruns of the last run
 };
 
 static const fk_tuning kDefaultTuning = {3, 3, 2048, (u32)kWarpMode,
                                          (u32)kSegPerTask, 8, 65536, 1.0f,
-                                         256};
+                                         256, 1.0f,
+                                         (float)kDefaultRoundCut};
 
 // Upload this batch's copy of every engine descriptor with the marked
 // prime range cut at tune.mark_limit, and the matching cost models.
@@ -611,6 +628,18 @@ static fk_status apply_tuning(fk_batch* b) {
   std::vector<DevEngine> de(ne);
   b->cost.assign(ne, Cost());
   b->mark_ok.assign(ne, 0);
+  // this batch's compaction-round cuts, every engine's in one buffer
+  std::vector<std::vector<u32>> rounds(ne);
+  std::vector<u32> flat;
+  for (u32 i = 0; i < ne; ++i) {
+    rounds[i] = compute_rounds(b->engines[i], b->tune.round_cut);
+    flat.insert(flat.end(), rounds[i].begin(), rounds[i].end());
+  }
+  fk_status rs = b->d_rounds.ensure(flat.size());
+  if (rs) return rs;
+  FK_CUDA(cudaMemcpy(b->d_rounds.p, flat.data(), flat.size() * sizeof(u32),
+                     cudaMemcpyHostToDevice));
+  size_t roff = 0;
   for (u32 i = 0; i < ne; ++i) {
     const fk_engine* e = b->engines[i];
     DevEngine d = e->dev;
@@ -621,6 +650,9 @@ static fk_status apply_tuning(fk_batch* b) {
     b->cost[i] = npm == e->dev.NPm ? e->cost : engine_cost(e, npm);
     b->mark_ok[i] = e->use_mark && npm > (u32)kNS;
     d.use_mark = b->mark_ok[i];
+    d.rounds = b->d_rounds.p + roff;
+    d.nrounds = (u32)rounds[i].size() - 1;
+    roff += rounds[i].size();
     de[i] = d;
   }
   FK_CUDA(cudaMemcpy(b->d_engines, de.data(), sizeof(DevEngine) * ne,
@@ -682,7 +714,7 @@ static void batch_free(fk_batch* b) {
   b->d_item_off.release(); b->d_sorted.release(); b->d_scratch.release();
   b->d_nb.release(); b->d_bcount.release(); b->d_bfill.release();
   b->d_nbuckets.release(); b->d_bbase.release(); b->d_boff.release();
-  b->d_task_ctr.release(); b->d_nitems.release();
+  b->d_task_ctr.release(); b->d_nitems.release(); b->d_rounds.release();
   for (auto& f : b->fam) { f.d_idx.release(); f.d_prefix.release(); }
   b->h_items.release(); b->h_ctr.release(); b->h_off.release();
   b->h_sorted.release(); b->h_small.release(); b->h_prefix.release();
@@ -710,6 +742,18 @@ static bool chain_fits(const fk_engine* e, u128 x_hi, u32 cap, bool dense) {
   return x < std::ldexp(1.0L, 127) && x + (long double)cap * (long double)e->d < lim;
 }
 
+namespace fk {
+fk_status check_interval(const fk_engine* e, const uint64_t lo[2],
+                         const uint64_t hi[2], uint32_t cap, bool dense) {
+  const u128 l = u128_of(lo), h = u128_of(hi);
+  if (h - l >= ((u128)1 << 63))
+    return set_err(FK_ERR_DOMAIN, "interval wider than 2^63");
+  if (!chain_fits(e, h, cap, dense))
+    return set_err(FK_ERR_DOMAIN, "values past 190 bits at " + u128_str(h));
+  return FK_OK;
+}
+}  // namespace fk
+
 // Expand user items into device items (launch-sized sub-ranges).
 static fk_status expand(fk_batch* b, const fk_item* items, u64 nitems) {
   b->user.assign(items, items + nitems);
@@ -727,12 +771,12 @@ static fk_status expand(fk_batch* b, const fk_item* items, u64 nitems) {
     const fk_engine* e = b->engines[it.engine];
     const u128 lo = u128_of(it.lo), hi = u128_of(it.hi);
     if (hi <= lo) continue;
-    if (hi - lo >= ((u128)1 << 63))
-      return set_err(FK_ERR_DOMAIN, "interval wider than 2^63");
     if (it.mode > MODE_DENSE) return set_err(FK_ERR_ARG, "bad mode");
     if (it.cap > 250) return set_err(FK_ERR_DOMAIN, "cap above 250");
-    if (!chain_fits(e, hi, std::max(it.cap, it.threshold), it.mode == MODE_DENSE))
-      return set_err(FK_ERR_DOMAIN, "values past 190 bits at " + u128_str(hi));
+    fk_status cs = check_interval(e, it.lo, it.hi,
+                                  std::max(it.cap, it.threshold),
+                                  it.mode == MODE_DENSE);
+    if (cs) return cs;
     if (it.mode == MODE_DENSE) {
       const u64 cnt = (u64)(hi - lo);
       if (cnt > (1ull << 26)) return set_err(FK_ERR_DOMAIN, "dense range above 2^26");
@@ -752,10 +796,7 @@ static fk_status expand(fk_batch* b, const fk_item* items, u64 nitems) {
     const u64 M = e->M;
     const u128 X0 = lo / M * M;
     const u128 periods = (hi - X0 + M - 1) / M;
-    // periods per device item: offsets u*M + R stay below 2^55
-    u64 umax = (u64)(((u128)1 << 55) / M);
-    umax = std::max<u64>(64, umax / 64 * 64);
-    umax = std::min<u64>(umax, 1ull << 36);
+    const u64 umax = item_periods_max(M);
     const u64 L = e->lanes.size();
     for (u128 s0 = 0; s0 < periods; s0 += umax) {
       const u64 U = (u64)std::min<u128>(umax, periods - s0);
@@ -833,7 +874,8 @@ static fk_status expand(fk_batch* b, const fk_item* items, u64 nitems) {
     const fk_engine* e = b->engines[di.engine];
     expect += (long double)di.U * e->lanes.size() * e->survival * 3.0L + 64;
   }
-  const u64 need = (u64)std::min<long double>(expect * 2 + 4096, (long double)(1ull << 28));
+  const u64 need = (u64)std::min<long double>(
+      expect * 2 * b->tune.capacity_scale + 4096, (long double)(1ull << 28));
   if (need > b->cand_cap) {
     if ((st = b->d_cand_key.ensure(need))) return st;
     if ((st = b->d_cand_item.ensure(need))) return st;
@@ -1124,11 +1166,13 @@ static fk_status batch_run(fk_batch* b, const fk_item* items, u64 nitems,
                            int use_graph) {
   fk_status st = expand(b, items, nitems);
   if (st) return st;
+  b->reruns = 0;
   for (int attempt = 0; attempt < 4; ++attempt) {
     if ((st = upload_items(b))) return st;
     if ((st = launch(b, use_graph))) return st;
     st = collect(b);
     if (st != FK_ERR_OVERFLOW) return st;
+    ++b->reruns;
   }
   return st;
 }
@@ -1263,8 +1307,10 @@ fk_status fk_batch_wait(fk_batch* b, fk_batch_result* out) {
   if (!b || !out) return set_err(FK_ERR_ARG, "null argument");
   if (!b->pending) return set_err(FK_ERR_ARG, "nothing pending");
   b->pending = false;
+  b->reruns = 0;
   fk_status st = collect(b);
   for (int attempt = 0; attempt < 3 && st == FK_ERR_OVERFLOW; ++attempt) {
+    ++b->reruns;
     if ((st = upload_items(b))) return st;
     if ((st = launch(b, b->pending_graph))) return st;
     st = collect(b);
@@ -1311,6 +1357,7 @@ static fk_status stats_of(const fk_batch* b, fk_stats* out) {
   out->marks = c.marks;
   out->h2d_bytes = b->h2d;
   out->d2h_bytes = b->d2h;
+  out->reruns = b->reruns;
   float a = 0, cl = 0, t = 0;
   FK_CUDA(cudaEventElapsedTime(&a, b->ev[0], b->ev[1]));
   FK_CUDA(cudaEventElapsedTime(&cl, b->ev[1], b->ev[2]));
@@ -1340,6 +1387,11 @@ fk_status fk_batch_set_tuning(fk_batch* b, const fk_tuning* t) {
   if (t->mark_limit) n.mark_limit = t->mark_limit;
   if (t->mark_bias > 0.0f) n.mark_bias = t->mark_bias;
   if (t->warp_lane_words) n.warp_lane_words = t->warp_lane_words;
+  if (t->capacity_scale > 0.0f) n.capacity_scale = t->capacity_scale;
+  if (t->round_cut > 0.0f) n.round_cut = t->round_cut;
+  if (!(n.capacity_scale >= 1e-4f && n.capacity_scale <= 1e3f) ||
+      !(n.round_cut >= 0.05f && n.round_cut <= 0.95f))
+    return set_err(FK_ERR_DOMAIN, "tuning value out of range");
   if (n.sieve_ctas_per_sm > 3 || n.mark_ctas_per_sm > 3 ||
       n.chains_per_sm < 64 || n.chains_per_sm > 65536 ||
       n.warp_queue > (u32)kWq + 1 || n.seg_per_task > 64 ||
@@ -1386,6 +1438,7 @@ EngineView engine_view(const fk_engine* e) {
   v.M = e->M;
   v.L = (uint32_t)e->lanes.size();
   v.NP = (uint32_t)e->sieve.size();
+  v.device = e->device;
   return v;
 }
 
@@ -1393,22 +1446,42 @@ fk_status set_error(fk_status s, const char* msg) { return set_err(s, msg); }
 }  // namespace fk
 
 // ------------------------------------------------------- peak probes ---
-// 32-bit multiply-add throughput: 8 independent lo/hi chains per thread.
+// Multiply throughput: 8 independent chains per thread.  MODE 0 alternates
+// mad.lo.u32 and mad.hi.u32 (the two halves of a CIOS word product), 1 is
+// mad.lo alone, 2 mad.hi alone, 3 mul.hi.u64 (the high half of a 64 x 64
+// product, as the sieve's Barrett reduction takes it).
+template <int MODE>
 __global__ void k_peak_imad(u32 seed, u32 iters, u32* sink) {
   u32 x[8];
+  u64 y[8];
 #pragma unroll
-  for (int i = 0; i < 8; ++i) x[i] = seed + threadIdx.x * 8 + i;
+  for (int i = 0; i < 8; ++i) {
+    x[i] = seed + threadIdx.x * 8 + i;
+    y[i] = ((u64)x[i] << 32) | (x[i] * 0x9e3779b9u);
+  }
   const u32 a = seed | 1u, c = seed ^ 0x9e3779b9u;
+  const u64 a64 = ((u64)a << 32) | 0x85ebca6bu;
   for (u32 it = 0; it < iters; ++it) {
 #pragma unroll
     for (int i = 0; i < 8; i += 2) {
-      asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(x[i]) : "r"(a), "r"(c));
-      asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(x[i + 1]) : "r"(a), "r"(c));
+      if (MODE == 0) {
+        asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(x[i]) : "r"(a), "r"(c));
+        asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(x[i + 1]) : "r"(a), "r"(c));
+      } else if (MODE == 1) {
+        asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(x[i]) : "r"(a), "r"(c));
+        asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(x[i + 1]) : "r"(a), "r"(c));
+      } else if (MODE == 2) {
+        asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(x[i]) : "r"(a), "r"(c));
+        asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(x[i + 1]) : "r"(a), "r"(c));
+      } else {
+        asm volatile("mul.hi.u64 %0, %0, %1;" : "+l"(y[i]) : "l"(a64));
+        asm volatile("mul.hi.u64 %0, %0, %1;" : "+l"(y[i + 1]) : "l"(a64));
+      }
     }
   }
   u32 r = 0;
 #pragma unroll
-  for (int i = 0; i < 8; ++i) r ^= x[i];
+  for (int i = 0; i < 8; ++i) r ^= x[i] ^ (u32)y[i] ^ (u32)(y[i] >> 32);
   if (r == 0x12345678u) sink[0] = r;
 }
 
@@ -1447,7 +1520,7 @@ __global__ void k_peak_smem_st(u32 iters, u32* sink) {
 
 extern "C" fk_status fk_peak(int which, double* per_second) {
   if (!per_second) return set_err(FK_ERR_ARG, "null argument");
-  if (which < 0 || which > 2) return set_err(FK_ERR_ARG, "which must be 0, 1 or 2");
+  if (which < 0 || which > 5) return set_err(FK_ERR_ARG, "which must be 0..5");
   int dev = 0, nsm = 0;
   FK_CUDA(cudaGetDevice(&dev));
   FK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -1456,12 +1529,19 @@ extern "C" fk_status fk_peak(int which, double* per_second) {
   cudaEvent_t e0, e1;
   FK_CUDA(cudaEventCreate(&e0));
   FK_CUDA(cudaEventCreate(&e1));
-  const u32 grid = nsm * 8, iters = which == 0 ? 1u << 16 : 1u << 14;
+  const bool mul = which == 0 || which >= 3;
+  const u32 grid = nsm * 8, iters = mul ? 1u << 16 : 1u << 14;
   float best = 1e30f;
   for (int rep = 0; rep < 4; ++rep) {
     FK_CUDA(cudaEventRecord(e0));
     if (which == 0)
-      k_peak_imad<<<grid, kBlock>>>(rep + 7, iters, (u32*)sink);
+      k_peak_imad<0><<<grid, kBlock>>>(rep + 7, iters, (u32*)sink);
+    else if (which == 3)
+      k_peak_imad<1><<<grid, kBlock>>>(rep + 7, iters, (u32*)sink);
+    else if (which == 4)
+      k_peak_imad<2><<<grid, kBlock>>>(rep + 7, iters, (u32*)sink);
+    else if (which == 5)
+      k_peak_imad<3><<<grid, kBlock>>>(rep + 7, iters, (u32*)sink);
     else if (which == 1)
       k_peak_smem<<<grid, kBlock>>>(iters, (u64*)sink);
     else
@@ -1476,7 +1556,7 @@ extern "C" fk_status fk_peak(int which, double* per_second) {
   cudaEventDestroy(e1);
   cudaFree(sink);
   const double threads = (double)grid * kBlock;
-  const double work = which == 0   ? threads * iters * 8.0        // IMADs
+  const double work = mul          ? threads * iters * 8.0        // products
                       : which == 1 ? threads * iters * 4.0 * 8.0  // bytes
                                    : threads * iters * 8.0;       // stores
   *per_second = work / (best * 1e-3);

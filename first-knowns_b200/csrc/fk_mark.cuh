@@ -72,48 +72,6 @@ struct PatSeg<P0, NS, NS> {
                                                u64&, u64&) {}
 };
 
-// Stage an engine's pattern table into shared memory with a bulk async
-// copy, bounded wait.  Returns false (and flags the counters) on timeout.
-template <int P0>
-__device__ __forceinline__ bool stage_patterns(u64* spat, const DevEngine& eg,
-                                               unsigned long long* mbar,
-                                               u32* status, u32& phase,
-                                               DevCounters* ctr) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    *status = 0;
-    const u32 mb = smem_u32(mbar);
-    const u32 bytes = pat_bytes<P0>();
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile(
-        "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb),
-        "r"(bytes)
-        : "memory");
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1], %2, [%3];" ::"r"(smem_u32(spat)),
-        "l"((u64)__cvta_generic_to_global(eg.pat)), "r"(bytes), "r"(mb)
-        : "memory");
-    u32 done = 0, spins = 0;
-    while (!done) {
-      asm volatile(
-          "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, "
-          "[%1], %2; selp.u32 %0, 1, 0, p; }"
-          : "=r"(done)
-          : "r"(mb), "r"(phase)
-          : "memory");
-      if (!done && ++spins > kWaitSpins) break;
-    }
-    if (!done) {
-      *status = 1;
-      atomicOr(&ctr->overflow, 4u);
-    }
-  }
-  phase ^= 1u;
-  __syncthreads();
-  return *status == 0;
-}
-
 template <int KIND>
 __device__ __forceinline__ bool tail_alive(u64 v, const DevEngine& e,
                                            const u32* __restrict__ xq,

@@ -16,10 +16,17 @@
 //
 // Limits (rejected with FK_ERR_DOMAIN and a message before any launch):
 //   * at most kMaxPrimes sieve primes (q2 up to about 821,000);
-//   * the interval must fit one device item (periods * M below 2^55);
-// and at run time, more than kMaxCand pre-primality survivors (or more
-// than the caller's capacity) is reported by writing UINT64_MAX to the
-// caller's count instead of a result.
+//   * the interval must fit one device item (periods * M below 2^55, the
+//     same bound fk_sieve cuts its items at: item_periods_max), on top of
+//     the domain checks every sweep applies (check_interval);
+// the current device must be the one the engine was created on
+// (FK_ERR_DEVICE otherwise, before any launch); and at run time the
+// caller's count receives, instead of a result,
+//   UINT64_MAX      more than kMaxCand pre-primality survivors, or more
+//                   than the caller's capacity (split the interval);
+//   UINT64_MAX - 1  a bounded device wait gave up (the pattern staging);
+//                   splitting the interval does not help -- the device is
+//                   stalled or faulty.
 //
 // Sharing: every call, from any thread, uses the same array on a given
 // device, and the array keeps the previous call's contents; each call
@@ -109,7 +116,11 @@ __global__ void __launch_bounds__(kBlock) k_na_finish(
     unsigned char* s, u64* out, u64 capacity, u64* count, u64 lo_shift) {
   const DevCounters* c = reinterpret_cast<const DevCounters*>(s + kOffCtr);
   const u64 n = c->ncand;
-  if (n > kMaxCand || n > capacity || (c->overflow & 5u)) {
+  if (c->overflow & 4u) {             // staging timeout: not a size issue
+    if (threadIdx.x == 0) *count = ~0ull - 1;
+    return;
+  }
+  if (n > kMaxCand || n > capacity || (c->overflow & 1u)) {
     if (threadIdx.x == 0) *count = ~0ull;
     return;
   }
@@ -163,19 +174,25 @@ extern "C" fk_status fk_sieve_noalloc(fk_engine* e, const uint64_t lo[2],
   const u128 H0 = ((u128)hi[1] << 64) | hi[0];
   if (H0 <= L0)
     return set_error(FK_ERR_DOMAIN, "fk_sieve_noalloc: empty interval");
+  fk_status cs = check_interval(e, lo, hi, 0, false);
+  if (cs) return cs;
   const u64 M = v.M;
   const u128 X0 = L0 / M * M;
   const u128 periods = (H0 - X0 + M - 1) / M;
-  u64 umax = (u64)(((u128)1 << 55) / M);
-  umax = umax / 64 * 64;
-  if (periods > (u128)umax || periods >= ((u128)1 << 36))
+  if (periods > (u128)item_periods_max(M))
     return set_error(FK_ERR_DOMAIN,
                      "fk_sieve_noalloc: interval too long for one call "
                      "(periods * M must stay below 2^55)");
-  // per-device set-up: the array's device address and kernel attributes
+  // the engine's tables must live on the current device
   int dev = 0;
   cudaError_t ce = cudaGetDevice(&dev);
   if (ce != cudaSuccess) return set_error(FK_ERR_DEVICE, cudaGetErrorString(ce));
+  {
+    char msg[192];
+    if (check_engine_device(v.device, dev, msg, sizeof msg))
+      return set_error(FK_ERR_DEVICE, msg);
+  }
+  // per-device set-up: the array's device address and kernel attributes
   if (dev < 0 || dev >= 64) return set_error(FK_ERR_DEVICE, "device index above 63");
   unsigned char* base = nullptr;
   {

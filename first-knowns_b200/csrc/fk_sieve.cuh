@@ -311,6 +311,57 @@ __device__ __forceinline__ void drain_any(u32* qin, u32* qout, u32 n,
   }
 }
 
+// Polls the CTA's mbarrier for the given phase, at most `spins` times.
+__device__ __forceinline__ bool mbar_wait(u32 mb, u32 phase, u32 spins) {
+  u32 done = 0;
+  for (u32 i = 0; i < spins && !done; ++i)
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, "
+        "[%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(mb), "r"(phase)
+        : "memory");
+  return done != 0;
+}
+
+// Stage an engine's pattern table into shared memory with one bulk async
+// copy (TMA) completing on the CTA's mbarrier, waiting a bounded number of
+// polls.  On a timeout it flags the counters (the host reports
+// FK_ERR_TIMEOUT) and returns false, after a second bounded wait for the
+// copy to land: the CTA then exits, and a copy still writing into the
+// shared memory of an exited CTA is what the second wait avoids.  Every
+// thread of the CTA calls it.
+template <int P0>
+__device__ __forceinline__ bool stage_patterns(u64* spat, const DevEngine& eg,
+                                               unsigned long long* mbar,
+                                               u32* status, u32& phase,
+                                               DevCounters* ctr) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *status = 0;
+    const u32 mb = smem_u32(mbar);
+    const u32 bytes = pat_bytes<P0>();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile(
+        "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb),
+        "r"(bytes)
+        : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1], %2, [%3];" ::"r"(smem_u32(spat)),
+        "l"((u64)__cvta_generic_to_global(eg.pat)), "r"(bytes), "r"(mb)
+        : "memory");
+    if (!mbar_wait(mb, phase, kWaitSpins)) {
+      *status = 1;
+      atomicOr(&ctr->overflow, 4u);
+      mbar_wait(mb, phase, kWaitSpins);  // let the copy in flight land
+    }
+  }
+  phase ^= 1u;
+  __syncthreads();
+  return *status == 0;
+}
+
 template <int P0>
 __global__ void __launch_bounds__(kBlock, 3) k_sieve(SieveArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -351,42 +402,12 @@ __global__ void __launch_bounds__(kBlock, 3) k_sieve(SieveArgs a) {
     const DevEngine& eg = a.engines[eidx];
     // ---- engine switch: stage its pattern table into shared memory ----
     if (S.eng != eidx) {
-      __syncthreads();
-      if (tid == 0) {
-        S.status = 0;
-        const u32 mb = smem_u32(&S.mbar);
-        const u32 bytes = pat_bytes<P0>();
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile(
-            "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb),
-            "r"(bytes)
-            : "memory");
-        asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
-            " [%0], [%1], %2, [%3];" ::"r"(smem_u32(spat)),
-            "l"((u64)__cvta_generic_to_global(eg.pat)), "r"(bytes), "r"(mb)
-            : "memory");
-        u32 done = 0, spins = 0;
-        while (!done) {
-          asm volatile(
-              "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, "
-              "[%1], %2; selp.u32 %0, 1, 0, p; }"
-              : "=r"(done)
-              : "r"(mb), "r"(phase)
-              : "memory");
-          if (!done && ++spins > kWaitSpins) break;
-        }
-        if (!done) {
-          S.status = 1;
-          atomicOr(&a.ctr->overflow, 4u);
-        }
-      }
+      if (!stage_patterns<P0>(spat, eg, &S.mbar, &S.status, phase, a.ctr))
+        return;
       for (u32 i = tid; i < kNS; i += kBlock) S.minv[i] = eg.pat_minv[i];
       for (u32 i = tid; i < eg.sbits_words && i < 512; i += kBlock)
         S.sbits[i] = eg.sbits[i];
-      phase ^= 1u;
       __syncthreads();
-      if (S.status) return;
       if (tid == 0) S.eng = eidx;
     }
     const DevEngine e = eg;

@@ -24,7 +24,7 @@ launch as the sieve.
 
 import functools
 
-from fk_abi import EULER, Engine
+from fk_abi import EULER, MODE_SIEVE, Batch, Engine
 
 WHEEL_PRIMES = [2, 3, 5, 7, 11, 13, 17, 19, 23]
 WHEEL_PRIMES_29 = WHEEL_PRIMES + [29]
@@ -90,6 +90,7 @@ class GpuEngine:
         self._mid = (_device_engine(self.n, 9) if self._p0_wide == 11
                      else None)
         self._narrow = _device_engine(self.n, 6)
+        self._batches = {}
 
     def _eng_for(self, lo, hi):
         # a window shorter than a few wide-wheel words wastes most lanes
@@ -108,12 +109,35 @@ class GpuEngine:
         return lo, hi
 
     def survivors_pre_mr(self, lo, hi, periods_per_launch=None):
-        """Sorted list of exact survivor p (Python ints) in [lo, hi)."""
+        """Sorted list of exact survivor p (Python ints) in [lo, hi).
+
+        With ``periods_per_launch`` the range is swept in launches of that
+        many periods of .M, as the reference's launches are
+        (euler-prime-runs/euler_gpu.py:1335-1456): each launch window is
+        one device item of a batch run, 256 launches per device call at
+        most.  The stream is the same either way."""
         lo, hi = self._check(lo, hi)
         if hi <= lo:
             return []
-        off = self._eng_for(lo, hi).sieve(lo, hi)
-        return [lo + int(o) for o in off.tolist()]
+        eng = self._eng_for(lo, hi)
+        if not periods_per_launch:
+            off = eng.sieve(lo, hi)
+            return [lo + int(o) for o in off.tolist()]
+        step = int(periods_per_launch) * self.M
+        if step <= 0:
+            raise ValueError("periods_per_launch must be positive")
+        if id(eng) not in self._batches:
+            self._batches[id(eng)] = Batch([eng])
+        b = self._batches[id(eng)]
+        starts = list(range(lo - lo % step, hi, step))
+        out = []
+        for g in range(0, len(starts), 256):
+            specs = [(0, MODE_SIEVE, 0, 0, max(lo, a), min(hi, a + step))
+                     for a in starts[g:g + 256]]
+            for (a, _m, _t, _c, wlo, _whi), (off, _d) in zip(
+                    specs, b.run(specs, graph=False)):
+                out.extend(wlo + int(o) for o in off.tolist())
+        return out
 
     def hunt(self, lo, hi, cap=100, periods_per_launch=None):
         """Ascending [(p, exact_run)] with run >= n in [lo, hi)."""

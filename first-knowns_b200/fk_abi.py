@@ -59,10 +59,10 @@ class Stats(ctypes.Structure):
                 ("marks", _u64), ("h2d_bytes", _u64), ("d2h_bytes", _u64),
                 ("sieve_ms", ctypes.c_float), ("classify_ms", ctypes.c_float),
                 ("total_ms", ctypes.c_float), ("mark_ms", ctypes.c_float),
-                ("rounds_ms", ctypes.c_float), ("pad", _u32)]
+                ("rounds_ms", ctypes.c_float), ("reruns", _u32)]
 
     def as_dict(self):
-        return {f: getattr(self, f) for f, _ in self._fields_ if f != "pad"}
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 class Tuning(ctypes.Structure):
@@ -70,7 +70,9 @@ class Tuning(ctypes.Structure):
                 ("chains_per_sm", _u32), ("warp_queue", _u32),
                 ("seg_per_task", _u32), ("classify_ctas_per_sm", _u32),
                 ("mark_limit", _u32), ("mark_bias", ctypes.c_float),
-                ("warp_lane_words", _u32)]
+                ("warp_lane_words", _u32),
+                ("capacity_scale", ctypes.c_float),
+                ("round_cut", ctypes.c_float)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -384,12 +386,15 @@ class Batch:
         return float(a.value), float(c.value), float(t.value)
 
 
+_FLOAT_FIELDS = ("mark_bias", "capacity_scale", "round_cut")
+
+
 def _tuning(kw):
     t = Tuning()
     for k, v in kw.items():
         if k not in TUNING_FIELDS:
             raise ValueError(f"unknown tuning field {k}")
-        setattr(t, k, float(v) if k == "mark_bias" else int(v))
+        setattr(t, k, float(v) if k in _FLOAT_FIELDS else int(v))
     return t
 
 
@@ -424,12 +429,17 @@ def set_device(device):
     _check(load().fk_set_device(int(device)))
 
 
+PEAKS = {"imad": 0, "smem": 1, "smem_st": 2, "imad_lo": 3, "imad_hi": 4,
+         "mul64hi": 5}
+
+
 def peak(which):
-    """Measured peak: 'imad' -> 32-bit multiply-adds/s, 'smem' -> shared
-    load bytes/s, 'smem_st' -> shared byte stores/s."""
+    """Measured peak: 'imad' -> 32-bit multiply-adds/s (mad.lo and mad.hi
+    alternating), 'imad_lo' / 'imad_hi' -> each half alone, 'mul64hi' ->
+    high halves of 64 x 64-bit products/s, 'smem' -> shared load bytes/s,
+    'smem_st' -> shared byte stores/s."""
     out = ctypes.c_double()
-    _check(load().fk_peak({"imad": 0, "smem": 1, "smem_st": 2}[which],
-                          ctypes.byref(out)))
+    _check(load().fk_peak(PEAKS[which], ctypes.byref(out)))
     return float(out.value)
 
 

@@ -6,9 +6,10 @@ SM when lanes are cut into chains, the compaction cadence (a warp's queue
 shorter than ``warp_queue`` goes one candidate per warp), the marking task length in
 32768-period segments, the lane length from which a warp sweeps one lane,
 the marking sieve's prime bound (primes below
-``mark_limit`` are marked, the rest tested per candidate) and the bias
-between marking and compaction rounds.  None of them can change a result;
-they only move time.
+``mark_limit`` are marked, the rest tested per candidate), the bias
+between marking and compaction rounds, and the survival at which a
+compaction round is cut (``round_cut``: lower means fewer, longer rounds).
+None of them can change a result; they only move time.
 
 ``tune`` runs coordinate descent: starting from the current setting it
 tries every value of one parameter at a time on a sample of the workload,
@@ -33,6 +34,7 @@ SPACE = {
     "mark_ctas_per_sm": [2, 3],
     "classify_ctas_per_sm": [4, 8, 16],
     "warp_lane_words": [64, 1024, 1 << 30],
+    "round_cut": [0.3, 0.7, 0.85],
 }
 
 DEFAULT_PATH = pathlib.Path(__file__).resolve().parent / "tuning.json"

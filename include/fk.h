@@ -171,6 +171,12 @@ typedef struct fk_tuning {
                                   * of the compaction rounds                   */
   uint32_t warp_lane_words;      /* lanes of at least this many 64-period      *
                                   * words are swept one warp per lane (>= 32)  */
+  float capacity_scale;          /* first candidate / output buffer size as a  *
+                                  * multiple of the survival model's estimate *
+                                  * (0.0001-1000): too small only costs a     *
+                                  * grow-and-rerun (fk_stats.reruns)           */
+  float round_cut;               /* a compaction round ends once survival     *
+                                  * within it falls below this (0.05-0.95)    */
 } fk_tuning;
 fk_status fk_batch_set_tuning(fk_batch* b, const fk_tuning* t);
 fk_status fk_batch_get_tuning(const fk_batch* b, fk_tuning* out);
@@ -195,7 +201,8 @@ typedef struct fk_stats {
   float sieve_ms, classify_ms, total_ms;
   float mark_ms;         /* device time of the marking-sieve launches       */
   float rounds_ms;       /* device time of the pattern + rounds launches    */
-  uint32_t pad;
+  uint32_t reruns;       /* pipeline reruns after a buffer overflow grew    *
+                          * the buffers (the result is the rerun's)         */
 } fk_stats;
 fk_status fk_batch_stats(const fk_batch* b, fk_stats* out);
 /* The same counters for an engine's last plain call. */
@@ -210,13 +217,19 @@ fk_status fk_engine_stats(const fk_engine* e, fk_stats* out);
  * entries) with their number in *d_count (a device uint64).  It allocates
  * nothing: all scratch lives in one fixed device array of about 5.3 MiB
  * that every GPU loading the library holds until exit.  Limits: at most
- * 65536 sieve primes and periods * M below 2^55 (else FK_ERR_DOMAIN), and
- * at most 262144 survivors per call -- more, or more than capacity, makes
- * *d_count UINT64_MAX.  Asynchronous on `stream` (a cudaStream_t, NULL for
- * the default stream): synchronise before reading the outputs.  Calls share
- * the array, so calls that overlap on the GPU race; serialise them.  The
- * first call on a device (with that device current) looks the array up;
- * make it before any stream capture.                                      */
+ * 65536 sieve primes and periods * M below 2^55, on top of fk_sieve's own
+ * domain checks (else FK_ERR_DOMAIN), and at most 262144 survivors per
+ * call.  The engine's device must be current (else FK_ERR_DEVICE, before
+ * any launch).  At run time *d_count receives the survivor count, or
+ *   UINT64_MAX      more than 262144 survivors, or more than capacity:
+ *                   split the interval and call again;
+ *   UINT64_MAX - 1  a bounded device wait gave up (pattern staging): a
+ *                   device fault or stall, which splitting does not cure.
+ * Asynchronous on `stream` (a cudaStream_t, NULL for the default stream):
+ * synchronise before reading the outputs.  Calls share the array, so calls
+ * that overlap on the GPU race; serialise them.  The first call on a
+ * device (with that device current) looks the array up; make it before
+ * any stream capture.                                                     */
 fk_status fk_sieve_noalloc(fk_engine* e, const uint64_t lo[2],
                            const uint64_t hi[2], uint64_t* d_offsets,
                            uint64_t capacity, uint64_t* d_count,
@@ -237,7 +250,9 @@ fk_status fk_set_device(int device);
 /* Measured device peaks for the rooflines: which = 0 gives 32-bit integer
  * multiply-adds per second (IMAD, lo and hi halves alternating), which = 1
  * shared-memory load bytes per second (64-bit, bank-conflict free),
- * which = 2 shared-memory byte stores per second (bank-conflict free). */
+ * which = 2 shared-memory byte stores per second (bank-conflict free),
+ * 3 mad.lo.u32 alone and 4 mad.hi.u32 alone per second, 5 mul.hi.u64
+ * (high half of a 64 x 64-bit product) per second.                     */
 fk_status fk_peak(int which, double* per_second);
 
 #ifdef __cplusplus

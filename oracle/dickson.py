@@ -134,6 +134,67 @@ class CpuEngine:
             return np.empty(0, dtype=np.uint64)
         return np.concatenate(parts)
 
+    def survivors_j_deep(self, j_lo, j_hi, block=1 << 22):
+        """Sorted surviving j in [j_lo, j_hi) as Python ints, at any depth.
+
+        The same strided marking as survivors_j with the segment base kept
+        as a Python int, so j may leave u64: the restatement of the deep
+        zone the reference's GPU engine reaches through survivors_j_deep
+        (dickson-ladders/ladder_gpu.py:783-804) and that its gate G17
+        checks against big-integer divisibility of the values themselves
+        (dickson-ladders/ladder_gpu.py:1206-1280; ``divisor`` below).  The
+        reference's CPU engine refuses j past J_CEIL only to keep its u64
+        output arrays exact (ladder_search.py:121-140 says so); nothing of
+        the mathematics changes there."""
+        j_lo, j_hi = int(j_lo), int(j_hi)
+        if j_lo * self.W < K_FLOOR:
+            raise ValueError("engines refuse to run below K_FLOOR")
+        out = []
+        j0 = j_lo
+        while j0 < j_hi:
+            j1 = min(j0 + block, j_hi)
+            alive = np.ones(j1 - j0, dtype=bool)
+            for q in self.primes:
+                s = j0 % q
+                for r in self.table[q]:
+                    first = int((int(r) - s) % q)
+                    if first < alive.size:
+                        alive[first::q] = False
+            out.extend(j0 + int(i) for i in np.nonzero(alive)[0].tolist())
+            j0 = j1
+        return out
+
+    def divisor(self, k):
+        """The first sieve prime dividing one of the values m*k^2 + 1,
+        m = 1..n, or None: the survivor definition itself, on Python ints,
+        as the reference's G17 evaluates it past u64 j
+        (dickson-ladders/ladder_gpu.py:1248-1255)."""
+        k = int(k)
+        for q in self.primes:
+            t = (k % q) * (k % q) % q
+            for m in range(1, self.n + 1):
+                if (m * t + 1) % q == 0:
+                    return q
+        return None
+
+    def hunt_deep(self, k_lo, k_hi, cap=None, min_run=None):
+        """hunt over [k_lo, k_hi] (inclusive) through survivors_j_deep, for
+        k past the u64 j ceiling; ``min_run`` (default n) is the least run
+        kept (ladder_search.py:150-162 keeps run >= n)."""
+        cap = cap or self.n + 8
+        want = self.n if min_run is None else int(min_run)
+        j_lo = max(1, -(-int(k_lo) // self.W))
+        j_hi = int(k_hi) // self.W + 1
+        out = []
+        for j in self.survivors_j_deep(j_lo, j_hi):
+            k = j * self.W
+            if k < k_lo or k > k_hi:
+                continue
+            r = run_length(k, cap=cap)
+            if r >= want:
+                out.append((k, r))
+        return out
+
     def survivors_pre_mr(self, k_lo, k_hi):
         """ladder_search.py:114-119: the stream on the k line, both ends
         inclusive."""

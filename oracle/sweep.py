@@ -9,7 +9,8 @@ return for one interval, in the search variable of the project:
   Euler    [lo, hi) in p: euler_search.CpuEngine(n).hunt(lo, hi, cap),
            with the launcher's low pass below P_FLOOR
   Dickson  [lo, hi) in k: ladder_search.CpuEngine(n, q2).hunt(lo, hi-1,
-           cap), with the low pass below K_FLOOR
+           cap), with the low pass below K_FLOOR, and the deep-zone sieve
+           (dickson.CpuEngine.hunt_deep) once j = k / W leaves J_CEIL
   AP       [lo, hi) in p: ap_search.CpuEngine(n, q2).hunt with the
            difference d (0: P(n)), chain cap ``cap``
 """
@@ -62,7 +63,11 @@ def hunt_interval(kind, n, lo, hi, threshold, cap, q2=65536, d=0):
                                         hi=min(hi, dickson.K_FLOOR)))
             lo = dickson.K_FLOOR
         if hi > lo:
-            out.extend(_dickson(n, q2).hunt(lo, hi - 1, cap=cap))
+            eng = _dickson(n, q2)
+            if (hi - 1) // eng.W + 1 > dickson.J_CEIL:
+                out.extend(eng.hunt_deep(lo, hi - 1, cap=cap))
+            else:
+                out.extend(eng.hunt(lo, hi - 1, cap=cap))
         return out
     eng = _ap(n, q2, d)
     return eng.hunt(lo, hi - lo, min_depth=threshold, cap=cap)

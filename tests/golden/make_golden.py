@@ -7,7 +7,7 @@ parity oracle for its GPU engines -- and freezes their outputs on the
 windows below as JSON.  The reference does not travel to the GPU host;
 these fixtures do.
 
-    python tests/golden/make_golden.py [/path/to/first-knowns]
+    python tests/golden/make_golden.py [/path/to/first-knowns] [--extras-only]
 
 Big integers are stored as decimal strings.  Sub-windows are swept in a
 process pool (``spawn``), and the result is the concatenation in window
@@ -104,6 +104,94 @@ def _ap_hunt(job):
             if dep >= min_depth:
                 out.append((p, dep))
     return out
+
+
+def _dickson_deep(job):
+    """Survivors of a window past u64 j by the reference's one-candidate
+    membership test (ladder_search.py:121-140 ``survives``, exact at any
+    j), with the reference's run length of each (ladder_search.py:
+    143-148) -- so every survivor's chain depth is frozen, hits or not."""
+    ref, n, q2, j_lo, j_hi, cap = job
+    _setup(ref)
+    import numpy as np
+    import ladder_search as ls
+    eng = ls.CpuEngine(n, q2=q2)
+    # candidates the reference's own residue table leaves for its primes
+    # below 2000 (strided, the way survivors_j marks); survives() then
+    # decides every one of them over all primes
+    alive = np.ones(j_hi - j_lo, dtype=bool)
+    for q in eng.primes:
+        if q >= 2000:
+            break
+        for r in eng.table[q]:
+            alive[int((int(r) - j_lo) % q)::q] = False
+    out = []
+    for t in np.nonzero(alive)[0].tolist():
+        j = j_lo + int(t)
+        if eng.survives(j):
+            out.append((j, eng.run_length(j * eng.W, cap=cap)))
+    return out
+
+
+# (n, q2, j_lo, span): the deep zone past u64 j, where the reference's
+# G17 gate checks its GPU stream against big-integer divisibility
+# (dickson-ladders/ladder_gpu.py:1206-1280), out to the served workload's
+# k ~ 1e24 (j = k / W up to about 5e21 at n = 6)
+DEEP_CASES = [(6, 65536, 2 ** 64 + 12345, 2 ** 20),
+              (6, 65536, 10 ** 21, 2 ** 20),
+              (6, 65536, 5 * 10 ** 21 - 2 ** 20, 2 ** 20),
+              (10, 65536, 2 ** 64, 2 ** 26),
+              (10, 4096, 5 * 10 ** 19, 2 ** 22),
+              (14, 4096, 2 ** 64 + 1, 2 ** 22),
+              (14, 2048, 3 * 10 ** 19, 2 ** 25),
+              (13, 2048, 17 * 4 * 10 ** 18 - 2 ** 22, 2 ** 22)]
+
+
+def dickson_deep(ref, pool):
+    out = {"cases": [], "source": "dickson-ladders/ladder_search.py:121-148 "
+                                  "survives and run_length of the reference"}
+    for n, q2, j_lo, span in DEEP_CASES:
+        parts = _split(j_lo, j_lo + span, 64)
+        cap = n + 8
+        res = pool.map(_dickson_deep, [(ref, n, q2, a, b, cap)
+                                       for a, b in parts])
+        rows = [r for rr in res for r in rr]
+        out["cases"].append({"n": n, "q2": q2, "j_lo": _s(j_lo),
+                             "j_hi": _s(j_lo + span), "cap": cap,
+                             "survivors": [_s(j) for j, _ in rows],
+                             "runs": [r for _, r in rows]})
+        print(f"dickson deep n={n} j={j_lo:.3g}: {len(rows)} survivors, "
+              f"max run {max((r for _, r in rows), default=0)}", flush=True)
+    (HERE / "dickson_deep.json").write_text(json.dumps(out))
+
+
+def cursor_units(ref):
+    """The values the launchers' checkpoint cursors are denominated in,
+    computed by the reference's own functions: the Euler wheel its engines
+    pick by default (euler_search.py:200-212 best_wheel; cursor key
+    euler-prime-runs/launch.py:191-200) and its period M, the Dickson wheel
+    modulus W (ladder_reference.py:60-66; next_j counts multiples of it,
+    dickson-ladders/launch.py:491-497, 604-610), and the AP engine floor
+    (ap_search.py:106; next_u starts at ceil(floor / 30),
+    primorial-ap/launch.py:262-273)."""
+    _setup(ref)
+    import ap_search as aps
+    import euler_search as es
+    import ladder_reference as lr
+    out = {"euler": {}, "dickson": {}, "ap_floor": {}}
+    for n in range(1, 21):
+        wp = list(es.best_wheel(n))
+        m = 1
+        for q in wp:
+            m *= q
+        out["euler"][str(n)] = {"wheel_primes": wp, "M": _s(m)}
+        out["dickson"][str(n)] = {"W": _s(lr.wheel_modulus(n))}
+    for q2 in (2048, 4096, 65536, 1 << 18):
+        out["ap_floor"][str(q2)] = _s(aps.CpuEngine(8, q2).floor)
+    out["source"] = ("euler_search.best_wheel, ladder_reference."
+                     "wheel_modulus, ap_search.CpuEngine.floor")
+    (HERE / "cursor.json").write_text(json.dumps(out, indent=1))
+    print("cursor units written", flush=True)
 
 
 def _split(lo, hi, parts, align=1):
@@ -346,9 +434,21 @@ def main(ref):
         },
     }
     (HERE / "known.json").write_text(json.dumps(known, indent=1))
+    dickson_deep(ref, pool)
+    cursor_units(ref)
     pool.close()
     print(f"done in {time.time()-t0:.0f}s")
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    ref_root = args[0] if args else "/root/reference"
+    if "--extras-only" in sys.argv:
+        # the deep-zone Dickson and cursor-unit fixtures alone
+        # (dickson_deep.json, cursor.json)
+        _setup(ref_root)
+        with mp.get_context("spawn").Pool(os.cpu_count() or 4) as pl:
+            dickson_deep(ref_root, pl)
+        cursor_units(ref_root)
+    else:
+        main(ref_root)

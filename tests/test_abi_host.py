@@ -124,3 +124,27 @@ def test_generated_montgomery_header_is_current(tmp_path, monkeypatch):
     gen.main()
     assert (tmp_path / "fk_mont32.cuh").read_text() == \
         (csrc / "fk_mont32.cuh").read_text()
+
+
+def test_noalloc_device_rule_rejects_a_foreign_device(tmp_path):
+    """fk_sieve_noalloc refuses to launch with an engine whose tables live
+    on another GPU than the current one (FK_ERR_DEVICE before any launch):
+    the check it calls, compiled host-only with g++ and driven on the CPU,
+    since a one-GPU machine cannot make the devices differ."""
+    import subprocess
+    import fk_abi
+    exe = tmp_path / "device_check"
+    src = ROOT / "tests" / "native" / "device_check.cpp"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-o", str(exe), str(src)],
+                   check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True,
+                         text=True).stdout.splitlines()
+    rows = [line.split(" ", 3) for line in out]
+    got = {(int(r[0]), int(r[1])): (int(r[2]), r[3] if len(r) > 3 else "")
+           for r in rows}
+    assert got[(0, 0)] == (fk_abi.FK_OK, "")
+    assert got[(7, 7)] == (fk_abi.FK_OK, "")
+    st, msg = got[(0, 1)]
+    assert st == fk_abi.FK_ERR_DEVICE and "device 0" in msg \
+        and "device 1 is current" in msg
+    assert got[(3, 2)][0] == fk_abi.FK_ERR_DEVICE

@@ -127,10 +127,13 @@ def test_tuning_changes_no_result():
                 dict(warp_queue=512, mark_bias=0.25),
                 dict(sieve_ctas_per_sm=1, mark_ctas_per_sm=1,
                      classify_ctas_per_sm=2),
+                dict(round_cut=0.7), dict(round_cut=0.2, warp_queue=64),
+                dict(round_cut=0.95, mark_bias=0.5),
                 dict(sieve_ctas_per_sm=3, mark_ctas_per_sm=3,
                      classify_ctas_per_sm=8, mark_limit=65536,
                      seg_per_task=8, warp_queue=32, mark_bias=1.0,
-                     chains_per_sm=2048, warp_lane_words=256)]
+                     chains_per_sm=2048, warp_lane_words=256,
+                     round_cut=0.5)]
     for kw in settings:
         be.set_tuning(**kw)
         assert _same(be.run_arrays(ivs, graph=True), ref), kw
@@ -139,6 +142,45 @@ def test_tuning_changes_no_result():
     assert _same(pe.run_arrays(ivs), ref)
     with pytest.raises(ValueError):
         be.set_tuning(mark_ctas_per_sm=9)
+    with pytest.raises(ValueError):
+        be.set_tuning(round_cut=0.99)
+
+
+def test_overflow_grows_the_buffers_and_reruns():
+    """First buffers sized far below the survival estimate overflow; the
+    pipeline grows them and reruns, and the rerun's stream is bit-identical
+    to a run that never overflowed: in fk_batch_run (graph and eager), in
+    fk_batch_submit / fk_batch_wait, and in the plain engine's fk_hunt."""
+    import fk_abi
+    from fk_batch import BatchEngine
+    ivs = _clipped(200, 83)
+    ref_be = BatchEngine(ivs)
+    ref = ref_be.run_arrays(ivs)
+    assert ref_be.stats()["reruns"] == 0
+    assert ref_be.stats()["candidates"] > 20000   # past the 4096 floor
+    for graph in (True, False):
+        small = BatchEngine(engset=ref_be.engset)
+        small.set_tuning(capacity_scale=1e-4)
+        assert _same(small.run_arrays(ivs, graph=graph), ref)
+        assert small.stats()["reruns"] >= 1
+        assert _same(small.run_arrays(ivs, graph=graph), ref)
+        assert small.stats()["reruns"] == 0       # grown buffers are kept
+    sw = BatchEngine(engset=ref_be.engset)
+    sw.set_tuning(capacity_scale=1e-4)
+    sw.submit(ivs)
+    assert _same(sw.wait_arrays(), ref)
+    assert sw.stats()["reruns"] >= 1
+    # the plain per-interval call on its own engine (Euler n = 4: about
+    # 1e-3 of the line survives, far past the 4096-entry floor)
+    lo, hi = 10 ** 12, 10 ** 12 + (1 << 26)
+    eng = fk_abi.Engine(fk_abi.EULER, 4, p0=6)
+    eng.set_tuning(capacity_scale=1e-4)
+    off, dep = eng.hunt(lo, hi, 0, 100)
+    assert eng.stats()["candidates"] > 8192 and eng.stats()["reruns"] >= 1
+    ref_eng = fk_abi.Engine(fk_abi.EULER, 4, p0=6)
+    roff, rdep = ref_eng.hunt(lo, hi, 0, 100)
+    assert ref_eng.stats()["reruns"] == 0
+    assert np.array_equal(off, roff) and np.array_equal(dep, rdep)
 
 
 def test_wide_wheel_intervals_match_the_narrow_wheel():

@@ -106,6 +106,27 @@ def test_dickson_low_pass():
     assert odk.low_pass(1, 12) == want
 
 
+@pytest.mark.parametrize("case", range(len(load("dickson_deep")["cases"])))
+def test_dickson_deep_zone(case):
+    """Past u64 j (up to j ~ 5e21, k ~ 1e24): the oracle's deep sieve and
+    run lengths equal the reference's survives() and run_length on the
+    same window, and every survivor passes the divisibility definition."""
+    c = load("dickson_deep")["cases"][case]
+    lo, hi = int(c["j_lo"]), int(c["j_hi"])
+    assert lo >= 1 << 64
+    eng = odk.CpuEngine(c["n"], c["q2"])
+    want = ints(c["survivors"])
+    for a, b in _subwindows(lo, hi, 1 << 22, 2, case, want):
+        got = eng.survivors_j_deep(a, b)
+        assert got == [j for j in want if a <= j < b]
+    runs = dict(zip(want, c["runs"]))
+    for j in want:
+        assert eng.divisor(j * eng.W) is None
+        assert odk.run_length(j * eng.W, cap=c["cap"]) == runs[j]
+    if c["n"] == 6:
+        assert len(want) > 100 and max(c["runs"]) >= 2
+
+
 # --------------------------------------------------------------------- AP --
 
 @pytest.mark.parametrize("case", range(len(load("ap")["surv"])))

@@ -7,7 +7,8 @@ is a fixed device array inside libfk.  These tests call it through the C
 ABI and require its result to equal the allocating entry point's
 (fk_sieve) exactly -- the streams are integer survivor offsets, so the
 tolerance is zero -- on two calls in a row, so the second call also shows
-that the shared array is reset between calls.
+that the shared array is reset between calls.  Every pattern family (p0)
+runs, and one case runs on a stream the caller created.
 
 This file is named to be collected last: if it fails, a run that stops
 at the first failure has already run every other test.
@@ -34,28 +35,36 @@ def _bind():
     return fk_abi, f
 
 
-def _call(f, fk_abi, eng, lo, hi, out, cnt, cap=CAP):
+def _call(f, fk_abi, eng, lo, hi, out, cnt, cap=CAP, stream=None):
     import torch
+    handle = stream.cuda_stream if stream is not None else None
     st = f(eng.handle, fk_abi.u128(lo), fk_abi.u128(hi), out.data_ptr(),
-           cap, cnt.data_ptr(), None)
+           cap, cnt.data_ptr(), handle)
+    if stream is not None:
+        stream.synchronize()
     torch.cuda.synchronize()
     return st
 
 
-def test_noalloc_equals_fk_sieve_on_two_calls_in_a_row():
+def _cases(p0):
+    import fk_abi
+    ap_lo = 4 * 10 ** 13 - (4 * 10 ** 13) % 30
+    out = [(fk_abi.Engine(fk_abi.EULER, 8, p0=p0), 10 ** 5, 10 ** 9)]
+    if p0 <= 9:            # the 31# wheel has too many AP / Dickson lanes
+        out += [(fk_abi.Engine(fk_abi.AP, 8, q2=4096, p0=p0), ap_lo,
+                 ap_lo + 3 * 10 ** 6),
+                (fk_abi.Engine(fk_abi.DICKSON, 6, q2=4096, p0=p0), 10 ** 6,
+                 10 ** 6 + 2 ** 20)]
+    return out
+
+
+@pytest.mark.parametrize("p0", [6, 7, 9, 11])
+def test_noalloc_equals_fk_sieve_on_two_calls_in_a_row(p0):
     import torch
     fk_abi, f = _bind()
     out = torch.zeros(CAP, dtype=torch.int64, device="cuda")
     cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
-    cases = [
-        (fk_abi.Engine(fk_abi.EULER, 8, p0=6), 10 ** 5, 10 ** 9),
-        (fk_abi.Engine(fk_abi.AP, 8, q2=4096, p0=6),
-         4 * 10 ** 13 - (4 * 10 ** 13) % 30,
-         4 * 10 ** 13 - (4 * 10 ** 13) % 30 + 3 * 10 ** 6),
-        (fk_abi.Engine(fk_abi.DICKSON, 6, q2=4096, p0=6), 10 ** 6,
-         10 ** 6 + 2 ** 20),
-    ]
-    for eng, lo, hi in cases:
+    for eng, lo, hi in _cases(p0):
         want = eng.sieve(lo, hi)
         assert want.size > 50
         for _ in range(2):                     # two calls in a row
@@ -66,6 +75,38 @@ def test_noalloc_equals_fk_sieve_on_two_calls_in_a_row():
             got = out[:n].cpu().numpy().view(np.uint64)
             assert n == want.size
             assert np.array_equal(got, want)
+
+
+def test_noalloc_on_a_caller_stream_near_the_survivor_limit():
+    """A call on a stream the caller created, with about 236,000
+    survivors (the array holds 262,144), timed with CUDA events on that
+    stream: the result equals fk_sieve's on two calls in a row."""
+    import torch
+    fk_abi, f = _bind()
+    eng = fk_abi.Engine(fk_abi.EULER, 2, p0=6)
+    lo, hi = 10 ** 12, 10 ** 12 + 7 * 10 ** 7
+    want = eng.sieve(lo, hi)
+    assert 150_000 < want.size < CAP
+    s = torch.cuda.Stream()
+    out = torch.zeros(CAP, dtype=torch.int64, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    times = []
+    for _ in range(2):
+        with torch.cuda.stream(s):
+            out.fill_(-1)
+            cnt.fill_(-1)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        assert _call(f, fk_abi, eng, lo, hi, out, cnt, stream=s) == 0
+        e1.record(s)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        n = int(cnt.item())
+        assert n == want.size
+        assert np.array_equal(out[:n].cpu().numpy().view(np.uint64), want)
+    print(f"fk_sieve_noalloc, {want.size} survivors: "
+          f"{min(times):.2f} ms per call")
 
 
 def test_noalloc_rejects_what_does_not_fit():
@@ -80,6 +121,9 @@ def test_noalloc_rejects_what_does_not_fit():
     eng = fk_abi.Engine(fk_abi.EULER, 8, p0=6)
     assert _call(f, fk_abi, eng, 10 ** 5, 10 ** 5, out, cnt) == \
         fk_abi.FK_ERR_DOMAIN                   # empty interval
+    assert _call(f, fk_abi, eng, 10 ** 5, 10 ** 5 + 2 ** 63, out, cnt) == \
+        fk_abi.FK_ERR_DOMAIN                   # wider than fk_sieve takes
     # more survivors than the caller's capacity: count reports UINT64_MAX
+    # (UINT64_MAX - 1 would mean a device wait gave up)
     assert _call(f, fk_abi, eng, 10 ** 5, 10 ** 9, out, cnt, cap=16) == 0
     assert int(cnt.item()) == -1
