@@ -131,7 +131,9 @@ struct fk_engine {
   std::vector<u64> lanes;
   std::vector<u32> sieve;     // pattern primes, then per-candidate primes
   std::vector<std::vector<u32>> forb;  // forbidden residues of x mod q
-  double survival = 1.0;      // expected survival through every sieve prime
+  double survival = 1.0;      // density of survivors on the line: the
+                              // product of 1 - f_q/q over the wheel and
+                              // every sieve prime (f_q forbidden residues)
   bool use_mark = false;      // long lanes go to the marking sieve
   bool force_mark = false;    // every item goes to the marking sieve
   std::vector<u32> mprefix;   // marking work entries before each marked prime
@@ -866,13 +868,15 @@ static fk_status expand(fk_batch* b, const fk_item* items, u64 nitems) {
   if (xo >= (1ull << 32) * 4) return set_err(FK_ERR_DOMAIN, "batch too large");
   fk_status st;
   if ((st = b->d_xq.ensure(xo + 16))) return st;
-  // capacities from the survival model
+  // capacities from the survival model: an item of U periods spans U*M
+  // of the line, of which a fraction `survival` survives the sieve; twice
+  // the expectation plus a floor per item absorbs the fluctuation
   long double expect = 0;
   for (size_t i = 0; i < b->items.size(); ++i) {
     const DevItem& di = b->items[i];
     if (di.mode == MODE_DENSE) { expect += di.U; continue; }
     const fk_engine* e = b->engines[di.engine];
-    expect += (long double)di.U * e->lanes.size() * e->survival * 3.0L + 64;
+    expect += (long double)di.U * e->M * e->survival + 64;
   }
   const u64 need = (u64)std::min<long double>(
       expect * 2 * b->tune.capacity_scale + 4096, (long double)(1ull << 28));
@@ -1219,6 +1223,7 @@ fk_status fk_engine_info(const fk_engine* e, fk_info* out) {
   out->device_bytes = e->device_bytes;
   out->use_mark = e->use_mark ? 1 : 0;
   out->marked_primes = e->dev.NPm > (u32)kNS ? e->dev.NPm - kNS : 0;
+  out->survival = e->survival;
   return FK_OK;
 }
 
@@ -1518,9 +1523,28 @@ __global__ void k_peak_smem_st(u32 iters, u32* sink) {
   if (buf[threadIdx.x] == 0xA5 && iters == 0) sink[0] = 1;
 }
 
+// Shared-memory bit marks: eight independent conflict-free red.shared.or.b32
+// per thread per trip (lane i of a warp on bank i), the store a bitmap
+// sieve would issue per mark.
+__global__ void k_peak_smem_or(u32 iters, u32* sink) {
+  __shared__ __align__(16) u32 buf[kBlock * 8];
+  for (int i = threadIdx.x; i < kBlock * 8; i += blockDim.x) buf[i] = 0;
+  __syncthreads();
+  const u32 base = (u32)__cvta_generic_to_shared(buf) + 4u * threadIdx.x;
+  for (u32 it = 0; it < iters; ++it) {
+#pragma unroll
+    for (u32 k = 0; k < 8; ++k)
+      asm volatile("red.shared.or.b32 [%0], %1;" ::"r"(base + k * 4u * kBlock),
+                   "r"(1u << (it & 31))
+                   : "memory");
+  }
+  __syncthreads();
+  if (buf[threadIdx.x] == 0xA5u && iters == 0) sink[0] = 1;
+}
+
 extern "C" fk_status fk_peak(int which, double* per_second) {
   if (!per_second) return set_err(FK_ERR_ARG, "null argument");
-  if (which < 0 || which > 5) return set_err(FK_ERR_ARG, "which must be 0..5");
+  if (which < 0 || which > 6) return set_err(FK_ERR_ARG, "which must be 0..6");
   int dev = 0, nsm = 0;
   FK_CUDA(cudaGetDevice(&dev));
   FK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -1544,6 +1568,8 @@ extern "C" fk_status fk_peak(int which, double* per_second) {
       k_peak_imad<3><<<grid, kBlock>>>(rep + 7, iters, (u32*)sink);
     else if (which == 1)
       k_peak_smem<<<grid, kBlock>>>(iters, (u64*)sink);
+    else if (which == 6)
+      k_peak_smem_or<<<grid, kBlock>>>(iters, (u32*)sink);
     else
       k_peak_smem_st<<<grid, kBlock>>>(iters, (u32*)sink);
     FK_CUDA(cudaEventRecord(e1));

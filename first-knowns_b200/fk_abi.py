@@ -39,7 +39,7 @@ class Info(ctypes.Structure):
     _fields_ = [("M", _u64), ("W", _u64), ("L", _u32), ("NP", _u32),
                 ("first_prime", _u32), ("nrounds", _u32),
                 ("device_bytes", _u64), ("use_mark", _u32),
-                ("marked_primes", _u32)]
+                ("marked_primes", _u32), ("survival", ctypes.c_double)]
 
 
 class Result(ctypes.Structure):
@@ -223,6 +223,7 @@ class Engine:
         self.device_bytes = int(inf.device_bytes)
         self.use_mark = bool(inf.use_mark)
         self.marked_primes = int(inf.marked_primes)
+        self.survival = float(inf.survival)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -430,14 +431,15 @@ def set_device(device):
 
 
 PEAKS = {"imad": 0, "smem": 1, "smem_st": 2, "imad_lo": 3, "imad_hi": 4,
-         "mul64hi": 5}
+         "mul64hi": 5, "smem_or": 6}
 
 
 def peak(which):
     """Measured peak: 'imad' -> 32-bit multiply-adds/s (mad.lo and mad.hi
     alternating), 'imad_lo' / 'imad_hi' -> each half alone, 'mul64hi' ->
     high halves of 64 x 64-bit products/s, 'smem' -> shared load bytes/s,
-    'smem_st' -> shared byte stores/s."""
+    'smem_st' -> shared byte stores/s, 'smem_or' -> shared bit marks
+    (red.shared.or.b32)/s."""
     out = ctypes.c_double()
     _check(load().fk_peak(PEAKS[which], ctypes.byref(out)))
     return float(out.value)

@@ -66,6 +66,9 @@ typedef struct fk_info {
   uint64_t device_bytes; /* bytes this engine holds on the device             */
   uint32_t use_mark;   /* long lanes use the marking sieve (cost model)      */
   uint32_t marked_primes; /* primes the marking sieve covers                 */
+  double survival;     /* expected pre-primality survivors per unit of the   *
+                        * line (product of 1 - f_q/q over the wheel and     *
+                        * sieve primes, f_q forbidden residues of q)        */
 } fk_info;
 
 /* One ordered result: x = base + offset[i]; depth[i] is the chain depth
@@ -252,7 +255,8 @@ fk_status fk_set_device(int device);
  * shared-memory load bytes per second (64-bit, bank-conflict free),
  * which = 2 shared-memory byte stores per second (bank-conflict free),
  * 3 mad.lo.u32 alone and 4 mad.hi.u32 alone per second, 5 mul.hi.u64
- * (high half of a 64 x 64-bit product) per second.                     */
+ * (high half of a 64 x 64-bit product) per second, 6 shared-memory bit
+ * marks (red.shared.or.b32, bank-conflict free) per second.            */
 fk_status fk_peak(int which, double* per_second);
 
 #ifdef __cplusplus

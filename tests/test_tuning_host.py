@@ -101,6 +101,9 @@ def test_ctypes_structs_follow_the_header():
         "fk_tuning")
     assert [f for f, _ in fk_abi.Stats._fields_] == _header_fields(
         "fk_stats")
+    assert [f for f, _ in fk_abi.Info._fields_] == _header_fields("fk_info")
+    assert [f for f, _ in fk_abi.Params._fields_] == _header_fields(
+        "fk_params")
     assert set(fk_abi.TUNING_FIELDS) >= set(__import__("fk_tune").SPACE)
 
 
