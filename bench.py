@@ -87,6 +87,8 @@ def parse():
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--tune-seconds", type=float, default=60.0)
     ap.add_argument("--no-scores", action="store_true")
+    ap.add_argument("--no-configs", action="store_true")
+    ap.add_argument("--plain-passes", type=int, default=3)
     ap.add_argument("--profile-case", default=None,
                     help="run one profiling case (PROFILE_CASES) and exit")
     ap.add_argument("--runs", type=int, default=2,
@@ -381,6 +383,96 @@ def reference_scores(runs=3):
     return out
 
 
+# --------------------------------------------------------------- serving ---
+
+def serve_bench(args):
+    """The served workload (Poisson arrivals; length 2^U(16,34), threshold
+    6..14, start 10^U(18,24)) through the continuous-batching loop.  The
+    arrival rate is 80% of the loop's measured capacity (256 requests
+    queued at once and served back to back give requests/s at full load).
+    Reports p50/p99 latency overall and per length class, the device-time
+    fraction, and the same arrivals through a single slot (no overlap)."""
+    import numpy as np
+    import fk_workloads as W
+    from fk_serve import ServeLoop
+    loop = ServeLoop(slots=2)
+    sample = [iv for _, iv in W.served(count=256, rate_hz=1.0,
+                                       seed=W.SEED + 7)]
+    loop.run([(0.0, iv) for iv in sample[:32]])        # warm: tables, buffers
+    _, _, cst = loop.run([(0.0, iv) for iv in sample])
+    capacity = len(sample) / cst["wall_s"]
+    rate = 0.8 * capacity
+    reqs = W.served(count=int(rate * args.serve_seconds * 1.5) + 64,
+                    rate_hz=rate)
+    lens = np.array([iv.length for _, iv in reqs], dtype=float)
+
+    def summary(lp, limit):
+        _, lat, st = lp.run(reqs, time_limit=limit)
+        done = ~np.isnan(lat)
+        out = {"requests": int(done.sum()),
+               "p50_ms": float(np.percentile(lat[done], 50) * 1e3),
+               "p99_ms": float(np.percentile(lat[done], 99) * 1e3),
+               "throughput": float(lens[done].sum() / st["wall_s"]),
+               "unit": UNIT, "batches": st["batches"],
+               "device_time_frac": st["device_busy_s"] / st["wall_s"]}
+        classes = {}
+        for name, lo, hi in (("short <2^22", 0, 2 ** 22),
+                             ("mid 2^22-2^28", 2 ** 22, 2 ** 28),
+                             ("long >=2^28", 2 ** 28, 2 ** 40)):
+            sel = done & (lens >= lo) & (lens < hi)
+            if sel.any():
+                classes[name] = {
+                    "requests": int(sel.sum()),
+                    "p50_ms": float(np.percentile(lat[sel], 50) * 1e3),
+                    "p99_ms": float(np.percentile(lat[sel], 99) * 1e3)}
+        out["by_length"] = classes
+        return out
+
+    two = summary(loop, args.serve_seconds)
+    one = summary(ServeLoop(engset=loop.engset, slots=1),
+                  args.serve_seconds / 2)
+    two.update({"arrival_hz": rate, "capacity_hz": capacity,
+                "rate_rule": "80% of the capacity measured with 256 "
+                             "requests queued at once",
+                "chunk": loop.chunk, "batch_work": loop.batch_work,
+                "one_slot": {k: one[k] for k in ("requests", "p50_ms",
+                                                 "p99_ms", "throughput",
+                                                 "device_time_frac")}})
+    return two
+
+
+def config_bench():
+    """The plain configurations, each swept whole by the plain engine
+    through the reference-API mirror (wall clock around one call, after a
+    warm-up call that builds the tables): Euler runs >= 8 over p < 1e9
+    (low pass + engine), Dickson depth >= 6 over k < 2^34 at q2 = 2^20, AP
+    13#-difference chains >= 10 over p in [1e12, 1e12 + 2^40)."""
+    import ap_gpu
+    import euler_gpu
+    import ladder_gpu
+    out = {}
+
+    def timed(name, span, fn, warm):
+        warm()
+        t0 = time.perf_counter()
+        hits = fn()
+        dt = time.perf_counter() - t0
+        out[name] = {"seconds": dt, "candidates": span,
+                     "value": span / dt, "unit": UNIT, "hits": len(hits)}
+
+    timed("euler_p_below_1e9_n8", 10 ** 9,
+          lambda: euler_gpu.sweep(2, 10 ** 9, 8, cap=64),
+          lambda: euler_gpu.sweep(2, 10 ** 6, 8, cap=64))
+    timed("dickson_k_below_2e34_n6", 2 ** 34,
+          lambda: ladder_gpu.sweep(1, 2 ** 34, 6, cap=8, q2=1 << 20),
+          lambda: ladder_gpu.sweep(1, 10 ** 8, 6, cap=8, q2=1 << 20))
+    aeng = ap_gpu.GpuEngine(10, 65536, d=30030)
+    timed("ap_13primorial_1e12_2e40_chains10", 2 ** 40,
+          lambda: aeng.hunt_cap(10 ** 12, 2 ** 40, 10, 16),
+          lambda: aeng.hunt_cap(10 ** 12, 2 ** 30, 10, 16))
+    return out
+
+
 # ------------------------------------------------------------ reference ---
 
 def bench_reference(args):
@@ -494,7 +586,10 @@ def bench_fk(args):
     st_mean = {k: statistics.mean(s[k] for s in stats)
                for k in ("sieve_ms", "classify_ms", "total_ms")}
 
-    # plain per-interval engine on the same intervals, bit-exact check
+    # plain per-interval engine on the same intervals (one fk_hunt call
+    # each, wall clock: the plain engine's own per-call overhead is part of
+    # what the batch removes), the median of `plain_passes` full passes,
+    # bit-exact against the batch
     plain = None
     bit_identical = None
     if not args.no_plain:
@@ -502,14 +597,18 @@ def bench_fk(args):
         pe.set_tuning(**tuning["setting"])
         pe.run_arrays(intervals[:64])          # warm
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        prow = pe.run_arrays(intervals)
-        tp = time.perf_counter() - t0
-        bit_identical = same(prow, ref_rows)
-        tp = dist.max(tp)
+        tps = []
+        bit_identical = True
+        for _ in range(max(1, args.plain_passes)):
+            t0 = time.perf_counter()
+            prow = pe.run_arrays(intervals)
+            tps.append(time.perf_counter() - t0)
+            bit_identical = bit_identical and same(prow, ref_rows)
+        tp = dist.max(statistics.median(tps))
         plain = {"value": cands * world / tp, "unit": UNIT,
-                 "ms_per_step": tp * 1e3,
-                 "calls": len(intervals)}
+                 "ms_per_step": tp * 1e3, "calls": len(intervals),
+                 "passes_ms": [round(t * 1e3, 1) for t in tps],
+                 "timing": "wall clock per pass, median of the passes"}
 
     # rooflines from the device work counters and measured peaks, one per
     # kernel; the dominant one (most device time) is `roofline`
@@ -567,37 +666,34 @@ def bench_fk(args):
     times = {"k_classify": cls_s, "k_mark": mark_s, "k_sieve": rnd_s}
     dominant = roofs[max(times, key=times.get)]
 
-    # CPU baseline (rank 0, one GPU): oracle on a bounded sample
+    # CPU baseline (rank 0, one GPU): oracle on a bounded sample, the
+    # median of three timed runs after a warm-up run
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         workers = os.cpu_count() or 1
         jobs = cpu_sample(intervals, workers)
         with cpu_pool(workers) as pool:
-            run_cpu(pool, jobs[:workers])       # build tables in workers
-            cc, dt, _ = run_cpu(pool, jobs)
+            run_cpu(pool, jobs)                 # build tables in workers
+            runs = [run_cpu(pool, jobs)[:2] for _ in range(3)]
+        cc = runs[0][0]
+        dt = statistics.median(r[1] for r in runs)
         cpu = {"value": cc / dt, "unit": UNIT, "cores": workers,
                "kind": "port",
                "sample": f"{len(jobs)} seeded intervals of the workload, "
-                         f"each clipped to 2^24: {cc:.4g} candidates in "
-                         f"{dt:.1f} s"}
+                         f"each clipped to 2^24: {cc:.4g} candidates, "
+                         f"median of 3 runs {dt:.2f} s "
+                         f"({', '.join(f'{r[1]:.2f}' for r in runs)})"}
 
     # served workload: continuous batching, p50/p99 latency
     serve = None
     if rank == 0 and world == 1 and not args.no_serve:
-        from fk_serve import ServeLoop
-        reqs = W.served(count=4000, rate_hz=250.0)
-        # the server keeps its own resident tables (the served requests'
-        # engines), created before the first arrival
-        loop = ServeLoop(slots=2)
-        res, lat, sst = loop.run(reqs, time_limit=args.serve_seconds)
-        done = ~np.isnan(lat)
-        served_c = sum(reqs[i][1].length for i in np.nonzero(done)[0])
-        serve = {"requests": int(done.sum()),
-                 "p50_ms": float(np.percentile(lat[done], 50) * 1e3),
-                 "p99_ms": float(np.percentile(lat[done], 99) * 1e3),
-                 "throughput": served_c / sst["wall_s"], "unit": UNIT,
-                 "arrival_hz": 250.0, "batches": sst["batches"],
-                 "device_busy_frac": sst["device_busy_s"] / sst["wall_s"]}
+        serve = serve_bench(args)
+
+    # the three plain configurations, whole, through the reference-API
+    # mirrors (one call each after a warm-up call on a short window)
+    plain_configs = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        plain_configs = config_bench()
 
     scores = None
     if rank == 0 and world == 1 and not args.no_scores:
@@ -631,6 +727,7 @@ def bench_fk(args):
             "bit_identical": bit_identical,
             "cpu_baseline": cpu,
             "serve": serve,
+            "plain_configs": plain_configs,
             "reference_scores": scores,
             "clocks": clk,
             "gpu_launches": int(st["launches"]) * args.steps,

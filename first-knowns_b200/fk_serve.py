@@ -1,21 +1,31 @@
 """Continuous-batching sweep server.
 
 Requests (engine kind, interval, threshold) arrive over time.  The loop
-keeps every device table resident (one ``EngineSet`` shared by all
-slots), and runs ``slots`` batch pipelines, each on its own CUDA stream:
-whenever a slot is free and requests are waiting, it admits as many as
-fit the slot's HBM budget and item limit and submits them, so requests
-that arrive while others are on the GPU start as soon as a slot frees up,
-and two batches overlap on the device.  A request's latency is the wall
-time from its arrival to its results being on the host.
+keeps every device table resident (one ``EngineSet`` shared by all slots)
+and runs ``slots`` batch pipelines, each on its own CUDA stream, so two
+batches overlap on the device while the host collects one and fills the
+other.
 
-Admission by footprint: a request is charged the bytes its run needs on
-the device -- the base-residue table of its engine (4 bytes per sieve
-prime) plus candidate and output slots sized by the engine's survival
-estimate -- and a batch admits requests while the sum stays under
-``hbm_budget``.  Results are bit-identical to running each request alone
-(the pipeline computes every interval independently); the tests check
-it.
+Requests are cut into chunks of at most ``chunk`` units of their engine's
+line variable (p, or j = k / W for Dickson) and queued chunk by chunk in
+arrival order.  Whenever a slot is free it takes queued chunks, oldest
+first, while the batch stays under a work budget (``batch_work`` line
+units) and an HBM budget, and submits them as one persistent launch; a
+request is answered when its last chunk comes back, its chunks' streams
+concatenated in order.  A long request therefore never holds a slot for
+long: short requests that arrive behind it join the next batch, and the
+device never idles while work is queued.
+
+Admission by footprint: a chunk is charged the device bytes its run needs
+-- the base-residue table of its engine (4 bytes per sieve prime) plus
+candidate and output slots for twice the survivors the engine's density
+predicts (``fk_info.survival``, the product of 1 - f_q/q over the wheel and
+sieve primes) -- and a batch admits chunks while the sum stays under
+``hbm_budget``.
+
+Results are bit-identical to sweeping each request alone with the plain
+engine: every chunk is an independent interval, and a request's chunks
+tile it (the tests check alone == in the mix == plain).
 """
 
 import collections
@@ -24,84 +34,150 @@ import time
 import numpy as np
 
 from fk_batch import BatchEngine, EngineSet
+from fk_workloads import DICKSON, Interval, line_range
 
-ENTRY_BYTES = 8 + 4 + 16 + 8 + 16   # candidate key/item, out rec, sorted, scratch
+# device bytes per candidate slot: key + item, output record, ordered copy,
+# ordering scratch
+ENTRY_BYTES = 8 + 4 + 16 + 8 + 16
 
 
 class ServeLoop:
     def __init__(self, engset=None, slots=2, max_items=256,
-                 hbm_budget=2 << 30):
+                 hbm_budget=2 << 30, chunk=1 << 30, batch_work=1 << 34):
         self.engset = engset or EngineSet()
         self.slots = [BatchEngine(engset=self.engset) for _ in range(slots)]
         self.max_items = int(max_items)
         self.hbm_budget = int(hbm_budget)
+        self.chunk = int(chunk)
+        self.batch_work = int(batch_work)
+
+    def _engine(self, iv):
+        return self.engset.get(self.engset.key_for(iv))
 
     def footprint(self, iv):
-        e = self.engset.get(self.engset.key_for(iv))
-        span = iv.length // (e.W if iv.kind == 1 else 1) + 1
-        # wheel density x survival estimate, with the pipeline's headroom
-        expect = span * e.L / max(e.M, 1) * 0.05 + 64
-        return 4 * e.NP + int(expect * 2) * ENTRY_BYTES + 256
+        """Device bytes a chunk's run needs (see the module docstring)."""
+        e = self._engine(iv)
+        lo, hi = line_range(iv, e.W if iv.kind == DICKSON else 1)
+        expect = (hi - lo) * e.survival + 64
+        return 4 * e.NP + int(2 * expect) * ENTRY_BYTES + 256
+
+    def chunks(self, iv):
+        """The request as intervals of at most `chunk` line units, in
+        order; each is an Interval of the same engine and threshold."""
+        W = self._engine(iv).W if iv.kind == DICKSON else 1
+        lo, hi = line_range(iv, W)
+        out = []
+        a = lo
+        while a < hi:
+            b = min(hi, a + self.chunk)
+            if iv.kind == DICKSON:   # back to k: [a*W, b*W) covers j in [a, b)
+                klo = iv.lo if a == lo else a * W
+                khi = iv.hi if b == hi else b * W
+                out.append(Interval(iv.kind, iv.n, klo, khi, iv.threshold,
+                                    iv.cap, iv.q2, iv.d))
+            else:
+                out.append(Interval(iv.kind, iv.n, a, b, iv.threshold,
+                                    iv.cap, iv.q2, iv.d))
+            a = b
+        return out or [iv]
 
     def run(self, requests, time_limit=None):
         """requests: [(arrival_s, Interval)] sorted by arrival.  Returns
-        (results per request, latency_s per request, stats)."""
+        (per request (offsets, depths) as the batch engine gives them for
+        the whole request, latency_s per request, stats)."""
         for _, iv in requests:
-            self.engset.get(self.engset.key_for(iv))   # tables resident up front
+            self._engine(iv)                    # tables resident up front
         for s in self.slots:
             s._ensure()
         n = len(requests)
+        parts = [None] * n                      # per request: chunk results
+        left = [0] * n                          # chunks still out
         results = [None] * n
         latency = np.full(n, np.nan)
-        waiting = collections.deque()
-        inflight = {}                          # slot index -> [request ids]
+        queue = collections.deque()             # (request, chunk index, iv)
+        inflight = {}                           # slot -> [(request, chunk, iv)]
         nxt = 0
         t0 = time.perf_counter()
         busy_s = 0.0
         batches = 0
-        while nxt < n or waiting or inflight:
+        work_done = 0
+        while nxt < n or queue or inflight:
             now = time.perf_counter() - t0
             if time_limit is not None and now > time_limit and not inflight:
                 break
             while nxt < n and requests[nxt][0] <= now:
-                waiting.append(nxt)
+                cs = self.chunks(requests[nxt][1])
+                parts[nxt] = [None] * len(cs)
+                left[nxt] = len(cs)
+                for ci, c in enumerate(cs):
+                    queue.append((nxt, ci, c))
                 nxt += 1
             # collect finished slots
             for si in list(inflight):
-                if self.slots[si]._batch.ready():
-                    ids = inflight.pop(si)
-                    rows = self.slots[si].wait_arrays()
-                    done = time.perf_counter() - t0
-                    st = self.slots[si].stats()
-                    busy_s += st["total_ms"] * 1e-3
-                    for rid, r in zip(ids, rows):
-                        results[rid] = r
-                        latency[rid] = done - requests[rid][0]
-            # admit into free slots
+                if not self.slots[si]._batch.ready():
+                    continue
+                done = inflight.pop(si)
+                rows = self.slots[si].wait_arrays()
+                st = self.slots[si].stats()
+                busy_s += st["total_ms"] * 1e-3
+                t_done = time.perf_counter() - t0
+                for (rid, ci, civ), row in zip(done, rows):
+                    parts[rid][ci] = (civ, row)
+                    left[rid] -= 1
+                    if left[rid] == 0:
+                        results[rid] = self._join(requests[rid][1],
+                                                  parts[rid])
+                        parts[rid] = None
+                        latency[rid] = t_done - requests[rid][0]
+            # fill free slots, oldest chunks first
             for si in range(len(self.slots)):
-                if si in inflight or not waiting:
+                if si in inflight or not queue:
                     continue
                 if time_limit is not None and now > time_limit:
                     break
-                ids, foot = [], 0
-                while waiting and len(ids) < self.max_items:
-                    f = self.footprint(requests[waiting[0]][1])
-                    if ids and foot + f > self.hbm_budget:
+                take, foot, work = [], 0, 0
+                while queue and len(take) < self.max_items:
+                    rid, ci, civ = queue[0]
+                    f = self.footprint(civ)
+                    e = self._engine(civ)
+                    lo, hi = line_range(civ, e.W if civ.kind == DICKSON
+                                        else 1)
+                    if take and (foot + f > self.hbm_budget or
+                                 work + (hi - lo) > self.batch_work):
                         break
-                    ids.append(waiting.popleft())
+                    take.append(queue.popleft())
                     foot += f
-                self.slots[si].submit([requests[i][1] for i in ids])
-                inflight[si] = ids
+                    work += hi - lo
+                self.slots[si].submit([c for _, _, c in take])
+                inflight[si] = take
                 batches += 1
-            if not waiting and nxt < n and not inflight:
-                # idle until the next arrival
+                work_done += work
+            if not queue and nxt < n and not inflight:
                 delay = requests[nxt][0] - (time.perf_counter() - t0)
                 if delay > 0:
-                    time.sleep(min(delay, 0.01))
+                    time.sleep(min(delay, 0.005))
             elif inflight:
-                time.sleep(0.0002)
+                time.sleep(0.0001)
         wall = time.perf_counter() - t0
         served = ~np.isnan(latency)
         stats = {"requests": int(served.sum()), "batches": batches,
-                 "wall_s": wall, "device_busy_s": busy_s}
+                 "wall_s": wall, "device_busy_s": busy_s,
+                 "line_units": work_done}
         return results, latency, stats
+
+    def _join(self, iv, parts):
+        """A request's (offsets, depths) from its chunks' rows: offsets are
+        relative to each chunk's start in the line variable, so they are
+        shifted to the request's start and concatenated in order."""
+        if len(parts) == 1:
+            return parts[0][1]
+        e = self._engine(iv)
+        W = e.W if iv.kind == DICKSON else 1
+        lo0, _ = line_range(iv, W)
+        offs, deps = [], []
+        for civ, (off, dep) in parts:
+            clo, _ = line_range(civ, W)
+            offs.append(off + np.uint64(clo - lo0))
+            deps.append(dep)
+        return (np.concatenate(offs).astype(np.uint64),
+                np.concatenate(deps).astype(np.uint8))

@@ -93,6 +93,30 @@ def test_serving_loop_matches_plain_results():
     assert _same(res, plain)
 
 
+def test_serving_loop_chunks_long_requests():
+    """Requests cut into many chunks (1/16 of their line each, spread over
+    several batches of a small work budget) come back identical to the
+    plain engine's single call on the whole request, Dickson (k = W*j)
+    included."""
+    import fk_workloads as W
+    from fk_batch import PlainEngine
+    from fk_serve import ServeLoop
+    reqs = []
+    for t, iv in W.served(count=40, rate_hz=2000.0, seed=W.SEED + 5):
+        hi = min(iv.hi, iv.lo + (1 << 26))
+        if iv.kind == W.AP:
+            hi = iv.lo + max(30, (hi - iv.lo) // 30 * 30)
+        reqs.append((t, W.Interval(iv.kind, iv.n, iv.lo, hi, 0, iv.cap)))
+    loop = ServeLoop(slots=2, chunk=1 << 22, batch_work=1 << 24)
+    pieces = [len(loop.chunks(iv)) for _, iv in reqs]
+    assert max(pieces) >= 8
+    res, lat, st = loop.run(reqs)
+    assert st["requests"] == len(reqs) and st["batches"] >= sum(pieces) // 8
+    plain = PlainEngine(loop.engset).run_arrays([iv for _, iv in reqs])
+    assert _same(res, plain)
+    assert sum(x[0].size for x in plain) > 1000
+
+
 def test_submit_ready_wait():
     import fk_abi
     from fk_batch import BatchEngine
