@@ -108,8 +108,11 @@ PROFILE_CASES = {
                      "chains on 122-bit values (four 32-bit limbs)",
     "sprp_served": "64 served-workload requests (starts 1e18-1e24) clipped "
                    "to 2^26: SPRP on up to 165-bit values",
-    "mixed": "256 intervals of the mixed workload, clipped to 2^28 (the "
-             "bench's kernel instances: k_sieve<7>, k_mark<7>, ...)",
+    "mixed": "256 intervals of the mixed workload, clipped to 2^28 (13# "
+             "wheel only: k_sieve<6>, k_mark<6>)",
+    "mixed_long": "48 intervals of the mixed workload at least 2^33 long, "
+                  "clipped to 2^34 (the 17# wheel's kernels, k_sieve<7> "
+                  "and k_mark<7>, which dominate the bench)",
     "euler_wide17": "the Euler n = 17 stream over [6.11e20, +2e15) through "
                     "the reference-API mirror (31# wheel; the SCORE_WIDE "
                     "window at a tenth of its length)",
@@ -134,6 +137,19 @@ def profile_intervals(name):
         return [W.Interval(W.DICKSON, 6, 10 ** 18 + i * 2 ** 36,
                            10 ** 18 + i * 2 ** 36 + 2 ** 34, 6, 14)
                 for i in range(8)]
+    if name == "mixed_long":
+        out = []
+        for iv in W.mixed_batch(4096):
+            if iv.length < 2 ** 33:
+                continue
+            hi = iv.lo + 2 ** 34
+            if iv.kind == W.AP:
+                hi -= (hi - iv.lo) % 30
+            out.append(W.Interval(iv.kind, iv.n, iv.lo, hi, iv.threshold,
+                                  iv.cap))
+            if len(out) == 48:
+                break
+        return out
     if name in ("mixed", "sprp_served"):
         src = (W.mixed_batch(256) if name == "mixed" else
                [iv for _, iv in W.served(count=64)])

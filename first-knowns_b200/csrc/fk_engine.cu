@@ -621,7 +621,7 @@ struct fk_batch {
 static const fk_tuning kDefaultTuning = {3, 3, 2048, (u32)kWarpMode,
                                          (u32)kSegPerTask, 8, 65536, 1.0f,
                                          256, 1.0f,
-                                         (float)kDefaultRoundCut};
+                                         (float)kDefaultRoundCut, 32};
 
 // Upload this batch's copy of every engine descriptor with the marked
 // prime range cut at tune.mark_limit, and the matching cost models.
@@ -835,20 +835,18 @@ static fk_status expand(fk_batch* b, const fk_item* items, u64 nitems) {
         u64 tc = (words * L + target_chains - 1) / target_chains;
         tc = std::min<u64>(std::max<u64>(tc, 1), 256);
         di.Tc = (u32)tc;
-        // long lanes: a warp per lane, its threads on interleaved words, so
-        // a warp's pattern loads are 32 consecutive table entries
-        di.warp_lanes = words >= (u64)b->tune.warp_lane_words;
-        if (di.warp_lanes) {
-          tc = std::min<u64>(tc, (words + 31) / 32);
-          di.Tc = (u32)tc;
-          di.nchunk = (words + 32 * tc - 1) / (32 * tc);
-          const u64 chains = di.nchunk * L;    // one per warp
-          di.ntask = (chains + kBlock / 32 - 1) / (kBlock / 32);
-        } else {
-          di.nchunk = (words + tc - 1) / tc;
-          const u64 chains = di.nchunk * L;
-          di.ntask = (chains + kBlock - 1) / kBlock;
-        }
+        // long lanes: a group of threads per lane (a warp, or eight
+        // threads for mid-length lanes), its threads on interleaved words,
+        // so a group's pattern loads are consecutive table entries
+        const u32 G = words >= (u64)b->tune.warp_lane_words ? 32u
+                      : words >= (u64)b->tune.group_lane_words ? 8u : 1u;
+        di.lane_threads = G;
+        tc = std::min<u64>(tc, (words + G - 1) / G);
+        di.Tc = (u32)tc;
+        di.nchunk = (words + G * tc - 1) / (G * tc);
+        const u64 chains = di.nchunk * L;      // one per group
+        const u64 per_task = kBlock / G;
+        di.ntask = (chains + per_task - 1) / per_task;
       }
       Family& f = b->fam[fam_of(e->P0, mark)];
       di.task0 = f.prefix.back();
@@ -1394,6 +1392,7 @@ fk_status fk_batch_set_tuning(fk_batch* b, const fk_tuning* t) {
   if (t->warp_lane_words) n.warp_lane_words = t->warp_lane_words;
   if (t->capacity_scale > 0.0f) n.capacity_scale = t->capacity_scale;
   if (t->round_cut > 0.0f) n.round_cut = t->round_cut;
+  if (t->group_lane_words) n.group_lane_words = t->group_lane_words;
   if (!(n.capacity_scale >= 1e-4f && n.capacity_scale <= 1e3f) ||
       !(n.round_cut >= 0.05f && n.round_cut <= 0.95f))
     return set_err(FK_ERR_DOMAIN, "tuning value out of range");
@@ -1401,7 +1400,7 @@ fk_status fk_batch_set_tuning(fk_batch* b, const fk_tuning* t) {
       n.chains_per_sm < 64 || n.chains_per_sm > 65536 ||
       n.warp_queue > (u32)kWq + 1 || n.seg_per_task > 64 ||
       n.classify_ctas_per_sm > 32 || n.mark_limit > 65536 ||
-      n.warp_lane_words < 32 ||
+      n.warp_lane_words < 32 || n.group_lane_words < 8 ||
       !(n.mark_bias < 1e6f))
     return set_err(FK_ERR_DOMAIN, "tuning value out of range");
   b->tune = n;

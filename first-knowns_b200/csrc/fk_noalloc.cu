@@ -227,6 +227,7 @@ extern "C" fk_status fk_sieve_noalloc(fk_engine* e, const uint64_t lo[2],
   u64 tc = (words * v.L + target - 1) / target;
   tc = tc < 1 ? 1 : (tc > 256 ? 256 : tc);
   it.Tc = (u32)tc;
+  it.lane_threads = 1;  // one lane per thread, Tc consecutive words
   it.nchunk = (words + tc - 1) / tc;
   const u64 ntask = (it.nchunk * v.L + kBlock - 1) / kBlock;
   it.ntask = ntask;

@@ -412,20 +412,22 @@ __global__ void __launch_bounds__(kBlock, 3) k_sieve(SieveArgs a) {
     }
     const DevEngine e = eg;
     // ---- this thread's chain -------------------------------------------
-    // thread layout: one lane per thread, Tc consecutive words; warp
-    // layout (long lanes): one lane per warp, thread t taking words
-    // t, t + 32, ... of a 32 * Tc word block
-    const bool wlay = it.warp_lanes != 0;
+    // G = lane_threads threads sweep one lane: thread t of the group takes
+    // words t, t + G, ... of a G * Tc word block, so a group's pattern
+    // loads are G consecutive table entries (G = 1: one lane per thread,
+    // Tc consecutive words; 8: four lanes per warp; 32: one per warp)
+    const u32 G = it.lane_threads;
+    const u32 gsh = G == 32 ? 5u : (G == 8 ? 3u : 0u);
     const u32 wl = tid & 31, wid = tid >> 5;
-    const u64 g = wlay ? (task - a.task_prefix[S.item]) * (kBlock / 32) + wid
-                       : (task - a.task_prefix[S.item]) * kBlock + tid;
+    const u64 g = (task - a.task_prefix[S.item]) * (u64)(kBlock >> gsh) +
+                  (tid >> gsh);
     const u64 nchain = it.nchunk * e.L;
     const bool active = g < nchain;
     const u64 chunk = active ? g / e.L : 0;
     const u32 lane = active ? (u32)(g % e.L) : 0;
     const u64 R = active ? e.lanes[lane] : 0;
-    const u64 w0 = wlay ? chunk * 32ull * it.Tc + wl : chunk * it.Tc;
-    const u32 stride = wlay ? 32u : 1u;
+    const u64 w0 = chunk * (u64)G * it.Tc + (tid & (G - 1));
+    const u32 stride = G;
     S.chain_R[tid] = R;
     S.chain_w0[tid] = w0;
     if (tid == 0) S.stride = stride;
@@ -451,8 +453,10 @@ __global__ void __launch_bounds__(kBlock, 3) k_sieve(SieveArgs a) {
       u64 sv[2] = {0, 0};
       if (active) {
         u64 acc[4] = {0, 0, 0, 0};
-        if (wlay)
+        if (G == 32)
           Pat<P0, 0, kNS>::template word2<32>(spat, rho, acc);
+        else if (G == 8)
+          Pat<P0, 0, kNS>::template word2<8>(spat, rho, acc);
         else
           Pat<P0, 0, kNS>::template word2<1>(spat, rho, acc);
 #pragma unroll

@@ -263,18 +263,30 @@ __device__ __forceinline__ void csub_n(u32* x, const u32* y) {
   for (int i = 0; i < N; ++i) x[i] = br ? x[i] : d[i];
 }
 
-// x = 2x mod m for x < m (the doubled value stays below R).
+// x = x - m when `carry` (a bit above the N words) is set or x >= m.
+template <int N>
+__device__ __forceinline__ void csub_c(u32* x, u32 carry, const u32* m) {
+  u32 d[N];
+  const u32 br = sub_n<N>(d, x, m);
+  const bool ge = carry || !br;
+#pragma unroll
+  for (int i = 0; i < N; ++i) x[i] = ge ? d[i] : x[i];
+}
+
+// x = 2x mod m for x < m (the bit shifted out of the top word counts).
 template <int N>
 __device__ __forceinline__ void dbl_n(u32* x, const u32* m) {
+  const u32 top = x[N - 1] >> 31;
 #pragma unroll
   for (int i = N - 1; i > 0; --i) x[i] = (x[i] << 1) | (x[i - 1] >> 31);
   x[0] <<= 1;
-  csub_n<N>(x, m);
+  csub_c<N>(x, top, m);
 }
 
-// r = a * b / R mod m in [0, 2m) for a, b < 2m and 4m < R = 2^(32N): CIOS
-// without the final subtraction (the result's top word stays zero).
-template <int N>
+// r = a * b / R mod m for R = 2^(32N), by CIOS.  Lazy (4m < R): a, b < 2m
+// give r < 2m with no final subtraction (the top word stays zero).
+// Strict: a, b < m give r < m after one conditional subtraction.
+template <int N, bool Strict = false>
 __device__ __forceinline__ void mul_n(u32* r, const u32* a, const u32* b,
                                       const u32* m, u32 minv) {
   u32 t[N + 2];
@@ -289,6 +301,7 @@ __device__ __forceinline__ void mul_n(u32* r, const u32* a, const u32* b,
     for (int j = 0; j < N + 1; ++j) t[j] = t[j + 1];
     t[N + 1] = 0;
   }
+  if (Strict) csub_c<N>(t, t[N], m);
 #pragma unroll
   for (int i = 0; i < N; ++i) r[i] = t[i];
 }
@@ -308,7 +321,10 @@ __device__ __forceinline__ void sel_n(u32* r, u32 w, const u32* t1,
   for (int i = 0; i < N; ++i) r[i] = w == 1 ? t1[i] : (w == 2 ? t2[i] : t3[i]);
 }
 
-template <int N>
+// One strong test on N words.  Lazy residues need 4m < R (bits <= 32N -
+// 2); Strict keeps every residue canonical and serves the 191- and 192-bit
+// values that six words hold without that margin.
+template <int N, bool Strict = false>
 __device__ __forceinline__ bool strong_n(const u32* m, u32 a, u64* imad) {
   u32 inv = m[0];
 #pragma unroll
@@ -363,11 +379,11 @@ __device__ __forceinline__ bool strong_n(const u32* m, u32 a, u64* imad) {
           t1[i] = (u32)x;
           c = (u32)(x >> 32);
         }
-        csub_n<N>(t1, m);
+        csub_c<N>(t1, c, m);
       }
     }
-    mul_n<N>(t2, t1, t1, m, minv);
-    mul_n<N>(t3, t2, t1, m, minv);
+    mul_n<N, Strict>(t2, t1, t1, m, minv);
+    mul_n<N, Strict>(t3, t2, t1, m, minv);
   }
   // the aligned bit pairs of d, top down; pairs never straddle a word
   u32 x[N];
@@ -380,15 +396,15 @@ __device__ __forceinline__ bool strong_n(const u32* m, u32 a, u64* imad) {
     for (int b = top | 1; b >= 1; b -= 2) {
       const u32 w = (dw >> (b - 1)) & 3u;
       if (started) {
-        mul_n<N>(x, x, x, m, minv);
-        mul_n<N>(x, x, x, m, minv);
+        mul_n<N, Strict>(x, x, x, m, minv);
+        mul_n<N, Strict>(x, x, x, m, minv);
         if (b2) {  // canonical first, then doublings mod m stay below m
           if (w) csub_n<N>(x, m);
           for (u32 k = 0; k < w; ++k) dbl_n<N>(x, m);
         } else if (w) {
           u32 y[N];
           sel_n<N>(y, w, t1, t2, t3);
-          mul_n<N>(x, x, y, m, minv);
+          mul_n<N, Strict>(x, x, y, m, minv);
         }
       } else {
         started = true;
@@ -407,7 +423,7 @@ __device__ __forceinline__ bool strong_n(const u32* m, u32 a, u64* imad) {
   csub_n<N>(x, m);
   if (eq_n<N>(x, one) || eq_n<N>(x, mone)) return true;
   for (int r = 1; r < s; ++r) {
-    mul_n<N>(x, x, x, m, minv);
+    mul_n<N, Strict>(x, x, x, m, minv);
     csub_n<N>(x, m);
     if (eq_n<N>(x, mone)) return true;
   }
@@ -415,7 +431,8 @@ __device__ __forceinline__ bool strong_n(const u32* m, u32 a, u64* imad) {
 }
 
 // The strong test of a value of 2^62 or more (three 64-bit limbs) to base
-// a, on N = ceil((bits + 2) / 32) 32-bit words, which keeps 4m < R.  Kept
+// a, on N = ceil((bits + 2) / 32) 32-bit words, which keeps 4m < R, or on
+// six words with canonical residues for 191 and 192 bits.  Kept
 // out of line, with scalars in and out, so the common one-word path of the
 // callers keeps its registers: returns the algorithmic IMADs << 1 | pass.
 __device__ __noinline__ u64 strong_wide(u64 w0, u64 w1, u64 w2, u32 a) {
@@ -431,7 +448,8 @@ __device__ __noinline__ u64 strong_wide(u64 w0, u64 w1, u64 w2, u32 a) {
   if (n <= 3) pass = strong_n<3>(w, a, &im);
   else if (n == 4) pass = strong_n<4>(w, a, &im);
   else if (n == 5) pass = strong_n<5>(w, a, &im);
-  else pass = strong_n<6>(w, a, &im);
+  else if (n == 6) pass = strong_n<6>(w, a, &im);
+  else pass = strong_n<6, true>(w, a, &im);
   return (im << 1) | (pass ? 1ull : 0ull);
 }
 

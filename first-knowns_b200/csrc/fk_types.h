@@ -80,8 +80,9 @@ struct DevItem {
   uint64_t lo_off;                // first valid x - X0 (in period 0)
   uint64_t hi_last;               // valid iff R < hi_last in period U-1
   uint32_t Tc;                    // words per chain (per thread)
-  uint32_t warp_lanes;            // 1: a warp sweeps one lane, thread t
-                                  // taking words t, t + 32, ...
+  uint32_t lane_threads;          // threads sweeping one lane: 1, 8 or 32;
+                                  // thread t of a group takes words t,
+                                  // t + lane_threads, ... of its block
   uint64_t nchunk;                // chains per lane
   uint64_t task0, ntask;          // first task, task count
   uint64_t xq_off;                // this item's base-residue table

@@ -5,7 +5,8 @@ persistent grids (pattern sieve + rounds, marking sieve, SPRP), chains per
 SM when lanes are cut into chains, the compaction cadence (a warp's queue
 shorter than ``warp_queue`` goes one candidate per warp), the marking task length in
 32768-period segments, the lane length from which a warp sweeps one lane,
-the marking sieve's prime bound (primes below
+the lane length from which eight threads sweep one lane
+(``group_lane_words``), the marking sieve's prime bound (primes below
 ``mark_limit`` are marked, the rest tested per candidate), the bias
 between marking and compaction rounds, and the survival at which a
 compaction round is cut (``round_cut``: lower means fewer, longer rounds).
@@ -35,6 +36,7 @@ SPACE = {
     "classify_ctas_per_sm": [4, 8, 16],
     "warp_lane_words": [64, 1024, 1 << 30],
     "round_cut": [0.3, 0.7, 0.85],
+    "group_lane_words": [16, 64, 1 << 30],
 }
 
 DEFAULT_PATH = pathlib.Path(__file__).resolve().parent / "tuning.json"

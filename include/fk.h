@@ -180,6 +180,9 @@ typedef struct fk_tuning {
                                   * grow-and-rerun (fk_stats.reruns)           */
   float round_cut;               /* a compaction round ends once survival     *
                                   * within it falls below this (0.05-0.95)    */
+  uint32_t group_lane_words;     /* lanes of at least this many words (and    *
+                                  * fewer than warp_lane_words) are swept by  *
+                                  * eight threads per lane (>= 8)             */
 } fk_tuning;
 fk_status fk_batch_set_tuning(fk_batch* b, const fk_tuning* t);
 fk_status fk_batch_get_tuning(const fk_batch* b, fk_tuning* out);

@@ -151,13 +151,15 @@ def test_tuning_changes_no_result():
                 dict(warp_queue=512, mark_bias=0.25),
                 dict(sieve_ctas_per_sm=1, mark_ctas_per_sm=1,
                      classify_ctas_per_sm=2),
+                dict(group_lane_words=1 << 30),
+                dict(group_lane_words=8, warp_lane_words=1 << 30),
                 dict(round_cut=0.7), dict(round_cut=0.2, warp_queue=64),
                 dict(round_cut=0.95, mark_bias=0.5),
                 dict(sieve_ctas_per_sm=3, mark_ctas_per_sm=3,
                      classify_ctas_per_sm=8, mark_limit=65536,
                      seg_per_task=8, warp_queue=32, mark_bias=1.0,
                      chains_per_sm=2048, warp_lane_words=256,
-                     round_cut=0.5)]
+                     round_cut=0.5, group_lane_words=32)]
     for kw in settings:
         be.set_tuning(**kw)
         assert _same(be.run_arrays(ivs, graph=True), ref), kw
@@ -194,14 +196,14 @@ def test_overflow_grows_the_buffers_and_reruns():
     sw.submit(ivs)
     assert _same(sw.wait_arrays(), ref)
     assert sw.stats()["reruns"] >= 1
-    # the plain per-interval call on its own engine (Euler n = 4: about
-    # 1e-3 of the line survives, far past the 4096-entry floor)
-    lo, hi = 10 ** 12, 10 ** 12 + (1 << 26)
-    eng = fk_abi.Engine(fk_abi.EULER, 4, p0=6)
+    # the plain per-interval call on its own engine (Euler n = 2: about
+    # 57,000 survivors in 2^24, far past the 4096-entry floor)
+    lo, hi = 10 ** 12, 10 ** 12 + (1 << 24)
+    eng = fk_abi.Engine(fk_abi.EULER, 2, p0=6)
     eng.set_tuning(capacity_scale=1e-4)
     off, dep = eng.hunt(lo, hi, 0, 100)
     assert eng.stats()["candidates"] > 8192 and eng.stats()["reruns"] >= 1
-    ref_eng = fk_abi.Engine(fk_abi.EULER, 4, p0=6)
+    ref_eng = fk_abi.Engine(fk_abi.EULER, 2, p0=6)
     roff, rdep = ref_eng.hunt(lo, hi, 0, 100)
     assert ref_eng.stats()["reruns"] == 0
     assert np.array_equal(off, roff) and np.array_equal(dep, rdep)

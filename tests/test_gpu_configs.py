@@ -111,4 +111,4 @@ def test_sub_windows_match_the_oracle(whole_line):
             [(p, d) for p, d in h5 if d >= N]
         n_surv += len(surv)
         n_hits += len(h5)
-    assert n_surv > 10000 and n_hits > 0
+    assert n_surv > 200 and n_hits > 0

@@ -88,10 +88,11 @@ def test_deep_zone_through_the_mirror():
 
 # ------------------------------------------- oracle, wider windows ---
 
-DEEP_WINDOWS = [(6, 65536, 2 ** 64 - 2 ** 21), (6, 65536, 3 * 10 ** 20),
-                (6, 65536, 5 * 10 ** 21), (10, 4096, 2 ** 64 + 99),
-                (10, 4096, 10 ** 21), (14, 4096, 7 * 10 ** 19),
-                (14, 4096, 3 * 10 ** 20)]
+# (n, q2, j_lo, log2 span): wide enough that each window holds survivors
+DEEP_WINDOWS = [(6, 65536, 2 ** 64 - 2 ** 21, 22), (6, 65536, 3 * 10 ** 20, 22),
+                (6, 65536, 5 * 10 ** 21, 22), (10, 4096, 2 ** 64 + 99, 22),
+                (10, 4096, 10 ** 21, 22), (14, 2048, 7 * 10 ** 19, 24),
+                (14, 2048, 3 * 10 ** 20, 24)]
 
 
 def _oracle_deep(job):
@@ -101,9 +102,9 @@ def _oracle_deep(job):
     return s, [odk.run_length(j * eng.W, cap) for j in s]
 
 
-@pytest.mark.parametrize("n,q2,lo", DEEP_WINDOWS)
-def test_deep_windows_match_the_oracle(n, q2, lo, sieve, pool):
-    span = 1 << 22
+@pytest.mark.parametrize("n,q2,lo,lspan", DEEP_WINDOWS)
+def test_deep_windows_match_the_oracle(n, q2, lo, lspan, sieve, pool):
+    span = 1 << lspan
     cap = n + 8
     parts = [(n, q2, lo + i * (span // 8), lo + (i + 1) * (span // 8), cap)
              for i in range(8)]

@@ -49,8 +49,13 @@ def _call(f, fk_abi, eng, lo, hi, out, cnt, cap=CAP, stream=None):
 def _cases(p0):
     import fk_abi
     ap_lo = 4 * 10 ** 13 - (4 * 10 ** 13) % 30
+    if p0 == 11:
+        # the 31# wheel fits n = 17 only (30 million lanes): the reference's
+        # SCORE window [1e16, 1e16 + 5e14), 178 survivors
+        return [(fk_abi.Engine(fk_abi.EULER, 17, p0=11), 10 ** 16,
+                 10 ** 16 + 5 * 10 ** 14)]
     out = [(fk_abi.Engine(fk_abi.EULER, 8, p0=p0), 10 ** 5, 10 ** 9)]
-    if p0 <= 9:            # the 31# wheel has too many AP / Dickson lanes
+    if p0 <= 9:
         out += [(fk_abi.Engine(fk_abi.AP, 8, q2=4096, p0=p0), ap_lo,
                  ap_lo + 3 * 10 ** 6),
                 (fk_abi.Engine(fk_abi.DICKSON, 6, q2=4096, p0=p0), 10 ** 6,
