@@ -59,6 +59,13 @@ def _device_engine(n, q2, d):
     return Engine(AP, n, q2=q2, p0=6, d=d)
 
 
+@functools.lru_cache(maxsize=None)
+def _device_batch(n, q2, d):
+    """One batch per device engine, shared by every GpuEngine of these
+    parameters (its buffers grow once and stay)."""
+    return Batch([_device_engine(n, q2, d)])
+
+
 class GpuEngine:
     """The primorial-step AP sieve + SPRP engine (reference API)."""
 
@@ -73,7 +80,6 @@ class GpuEngine:
         self.floor = max(P_FLOOR, self.q2)
         self._dev = _device_engine(self.n, self.q2, self.d)
         self._primes = None
-        self._batch = None
 
     @property
     def primes(self):
@@ -109,14 +115,13 @@ class GpuEngine:
         if span <= 0:
             return
         step = W0 * int(launch_u or self.launch_u)
-        if self._batch is None:
-            self._batch = Batch([self._dev])
+        batch = _device_batch(self.n, self.q2, self.d)
         starts = list(range(0, span, step))
         for g in range(0, len(starts), LAUNCHES_PER_CALL):
             group = starts[g:g + LAUNCHES_PER_CALL]
             specs = [(0, MODE_SIEVE, 0, 0, base + a, base + min(span, a + step))
                      for a in group]
-            rows = self._batch.run(specs, graph=False)
+            rows = batch.run(specs, graph=False)
             for a, (off, _dep) in zip(group, rows):
                 if off.size:
                     yield off + np.uint64(a)
