@@ -214,35 +214,7 @@ __device__ __forceinline__ bool lane_decide(LaneState& s, const ClassArgs& a) {
   return true;
 }
 
-// Advance a lane's state machine by the verdict of its current step;
-// returns whether the lane still holds a candidate.
-__device__ __forceinline__ bool lane_advance(LaneState& st, const ClassArgs& a,
-                                             bool pass) {
-  if (st.phase == 0) {
-    if (pass && st.t + 1 < st.lim) {
-      ++st.t;
-      return true;
-    }
-    st.d2 = pass ? st.lim : st.t;
-    return lane_decide(st, a);
-  }
-  if (!pass) {
-    lane_final(st, a, st.t);
-    return false;
-  }
-  if (st.bi < 6) {
-    ++st.bi;
-  } else if (st.t + 1 < st.d2) {
-    ++st.t;
-    st.bi = 1;
-  } else {
-    lane_final(st, a, st.d2);
-    return false;
-  }
-  return true;
-}
-
-__global__ void __launch_bounds__(kBlock, 2) k_classify(ClassArgs a) {
+__global__ void __launch_bounds__(kBlock) k_classify(ClassArgs a) {
   u64 n = a.ctr->ncand;
   if (n > a.cand_cap) n = a.cand_cap;
   const u32 lane = threadIdx.x & 31;
@@ -250,48 +222,53 @@ __global__ void __launch_bounds__(kBlock, 2) k_classify(ClassArgs a) {
   u64 chunk_pos = 0, chunk_end = 0;  // warp-uniform
   bool active = false, drained = false;
   LaneState st;
-  V3 v = {{0, 0, 0}};
   u64 imad = 0, nval = 0;
   for (;;) {
-    // Hand candidates to idle lanes and settle every step that trial
-    // division decides, until each lane holds a step that needs a strong
-    // test (or the candidates are gone): the warp's exponentiations then
-    // run with no lane idling on a value a small prime divides.
-    for (;;) {
-      while (!drained) {
-        const u32 idle = __ballot_sync(0xffffffffu, !active);
-        if (!idle) break;
-        if (chunk_pos >= chunk_end) {
-          unsigned long long base = 0;
-          if (lane == 0) base = atomicAdd(&a.ctr->class_next, (u64)kClassChunk);
-          base = __shfl_sync(0xffffffffu, base, 0);
-          if (base >= n) {
-            drained = true;
-            break;
-          }
-          chunk_pos = base;
-          chunk_end = min(base + (u64)kClassChunk, n);
+    // hand new candidates to idle lanes
+    while (!drained) {
+      const u32 idle = __ballot_sync(0xffffffffu, !active);
+      if (!idle) break;
+      if (chunk_pos >= chunk_end) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(&a.ctr->class_next, (u64)kClassChunk);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) {
+          drained = true;
+          break;
         }
-        const u32 rank = __popc(idle & lt);
-        const u32 take = (u32)min((u64)__popc(idle), chunk_end - chunk_pos);
-        if (!active && rank < take) active = lane_init(st, a, chunk_pos + rank);
-        chunk_pos += take;
+        chunk_pos = base;
+        chunk_end = min(base + (u64)kClassChunk, n);
       }
-      bool moved = false;
-      if (active) {
-        v = chain_value(st.c, st.t);
-        const int tr = sprp_trial(v);
-        if (tr != 2) {
-          active = lane_advance(st, a, tr == 1);
-          moved = true;
-        }
-      }
-      if (!__any_sync(0xffffffffu, moved)) break;
+      const u32 rank = __popc(idle & lt);
+      const u32 take = (u32)min((u64)__popc(idle), chunk_end - chunk_pos);
+      if (!active && rank < take) active = lane_init(st, a, chunk_pos + rank);
+      chunk_pos += take;
     }
     if (__ballot_sync(0xffffffffu, active) == 0) break;
     if (active) {
       ++nval;
-      active = lane_advance(st, a, sprp_strong(v, (int)st.bi, &imad));
+      const bool pass = sprp_step(chain_value(st.c, st.t), st.bi, &imad);
+      if (st.phase == 0) {
+        if (pass && st.t + 1 < st.lim) {
+          ++st.t;
+        } else {
+          st.d2 = pass ? st.lim : st.t;
+          active = lane_decide(st, a);
+        }
+      } else {
+        if (!pass) {
+          lane_final(st, a, st.t);
+          active = false;
+        } else if (st.bi < 6) {
+          ++st.bi;
+        } else if (st.t + 1 < st.d2) {
+          ++st.t;
+          st.bi = 1;
+        } else {
+          lane_final(st, a, st.d2);
+          active = false;
+        }
+      }
     }
   }
   // one atomic per warp for the work counters

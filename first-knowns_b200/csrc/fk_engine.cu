@@ -402,6 +402,7 @@ static fk_status build_engine(fk_engine* e) {
   }
   std::vector<PrimeRec> recs(NP);
   std::vector<u32> c64(NP), lists;
+  std::vector<u64> hmask(NP, 0);
   for (u32 i = 0; i < NP; ++i) {
     const u32 q = e->sieve[i];
     PrimeRec r;
@@ -418,10 +419,20 @@ static fk_status build_engine(fk_engine* e) {
       r.aux = dq ? (u32)invmod(dq, q) : 0;
     }
     if (use_list && i >= (u32)kNS) {
-      if (f.size() > 127) return set_err(FK_ERR_DOMAIN, "forbidden list too long");
+      std::vector<u32> lf = f;
+      if (e->kind == KIND_DICKSON) {
+        // the roots come in pairs x, q - x: keep min(x, q - x) and a 64-bit
+        // filter of the kept values mod 64
+        lf.clear();
+        for (u32 x : f) lf.push_back(std::min(x, q - x));
+        std::sort(lf.begin(), lf.end());
+        lf.erase(std::unique(lf.begin(), lf.end()), lf.end());
+        for (u32 h : lf) hmask[i] |= 1ull << (h & 63);
+      }
+      if (lf.size() > 127) return set_err(FK_ERR_DOMAIN, "forbidden list too long");
       if (lists.size() >= (1u << 24)) return set_err(FK_ERR_DOMAIN, "lists too large");
-      r.aux = 0x80000000u | ((u32)f.size() << 24) | (u32)lists.size();
-      lists.insert(lists.end(), f.begin(), f.end());
+      r.aux = 0x80000000u | ((u32)lf.size() << 24) | (u32)lists.size();
+      lists.insert(lists.end(), lf.begin(), lf.end());
     }
     recs[i] = r;
   }
@@ -496,6 +507,7 @@ static fk_status build_engine(fk_engine* e) {
   if ((st = upload(e, recs, &d.recs))) return st;
   if ((st = upload(e, c64, &d.c64))) return st;
   if ((st = upload(e, lists, &d.lists))) return st;
+  if ((st = upload(e, hmask, &d.hmask))) return st;
   if ((st = upload(e, rounds, &d.rounds))) return st;
   if ((st = upload(e, sbits, &d.sbits))) return st;
   d.NPm = NPm;

@@ -81,7 +81,9 @@ __device__ __forceinline__ bool tail_alive(u64 v, const DevEngine& e,
     u32 rr = fk_bmod(v, pr.q, pr.magic) + __ldg(xq + i);
     rr = min(rr, rr - pr.q);
     ++ntest;
-    if (kill_test<KIND>(pr, rr, e.lists, s_sbits, e.xxmax, e.n)) return false;
+    const u64 hm = KIND == KIND_DICKSON ? __ldg(e.hmask + i) : 0ull;
+    if (kill_test<KIND>(pr, rr, e.lists, s_sbits, e.xxmax, e.n, hm))
+      return false;
   }
   return true;
 }

@@ -38,6 +38,7 @@
 namespace fk {
 
 constexpr u32 kWaitSpins = 1u << 20;
+constexpr int kRoundUnroll = 4;  // primes per trip of the compaction rounds
 
 __device__ __forceinline__ u32 smem_u32(const void* p) {
   return (u32)__cvta_generic_to_shared(p);
@@ -81,7 +82,15 @@ template <int KIND>
 __device__ __forceinline__ bool kill_test(const PrimeRec& pr, u32 r,
                                           const u32* __restrict__ lists,
                                           const u32* s_sbits, u32 xxmax,
-                                          u32 n) {
+                                          u32 n, u64 hm) {
+  if (KIND == KIND_DICKSON) {
+    // the forbidden residues come in pairs r, q - r: h = min(r, q - r)
+    // must be on the half list, which a 64-bit filter of h mod 64
+    // screens first
+    const u32 h = min(r, pr.q - r);
+    if (!((hm >> (h & 63)) & 1ull)) return false;
+    return list_kill(pr.aux, h, lists);
+  }
   if (pr.aux & 0x80000000u) return list_kill(pr.aux, r, lists);
   if (KIND == KIND_EULER) {
     // q > max(x^2+x): r is killed iff q - r (mod q) is one of the x^2+x.
@@ -93,7 +102,10 @@ __device__ __forceinline__ bool kill_test(const PrimeRec& pr, u32 r,
     // j = (q - r) * d^-1 mod q is below n; aux = d^-1 (0 when q | d).
     if (r == 0) return true;
     if (pr.aux == 0) return false;
-    const u32 t = fk_mulmod(pr.q - r, pr.aux, pr.q, pr.magic);
+    // (q - r) * d^-1 < q^2 < 2^32: a 32-bit Barrett with floor(2^32 / q)
+    const u32 x = (pr.q - r) * pr.aux;
+    u32 t = x - __umulhi(x, (u32)(pr.magic >> 32)) * pr.q;
+    t = min(t, t - pr.q);
     return t < n;
   }
   return false;  // Dickson primes always carry a list
@@ -163,6 +175,24 @@ struct SieveArgs {
                       // candidate per warp
   u32 seg_per_task;   // marking: segments per task
 };
+
+// The entry of the item holding task t: the last i with task_prefix[i] <=
+// t, searched forward from `from` (a CTA's claims only grow, so its next
+// task's item is at or after its last one): a few steps, then bisection.
+__device__ __forceinline__ u32 task_item(const SieveArgs& a, u64 t, u32 from) {
+  u32 lo = from;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (lo + 1 < a.nitems && a.task_prefix[lo + 1] <= t) ++lo;
+    else return lo;
+  }
+  u32 hi = a.nitems;
+  while (hi - lo > 1) {
+    const u32 mid = (lo + hi) >> 1;
+    if (a.task_prefix[mid] <= t) lo = mid; else hi = mid;
+  }
+  return lo;
+}
 
 // Per-warp candidate queues: kQcap / 8 entries per warp, two buffers.
 constexpr u32 kWq = kQcap / (kBlock / 32);
@@ -239,7 +269,8 @@ __device__ void warp_drain(u32* qin, u32* qout, u32 n, const SieveSmem& S,
             const PrimeRec pr = e.recs[i];
             u32 rr = fk_bmod(v, pr.q, pr.magic) + __ldg(xq + i);
             rr = min(rr, rr - pr.q);
-            kill = kill_test<KIND>(pr, rr, e.lists, S.sbits, e.xxmax, e.n);
+            const u64 hm = KIND == KIND_DICKSON ? __ldg(e.hmask + i) : 0ull;
+            kill = kill_test<KIND>(pr, rr, e.lists, S.sbits, e.xxmax, e.n, hm);
             ++ntest;
           }
           dead = __any_sync(0xffffffffu, kill);
@@ -260,11 +291,39 @@ __device__ void warp_drain(u32* qin, u32* qout, u32 n, const SieveSmem& S,
         const u64 v = cand_value(S, code, M);
         alive = true;
         u32 i = i0;
-        for (; i < i1; ++i) {
+        // kRoundUnroll primes per trip, every load issued before any test
+        // (a kill ends the round; tests past it in the trip are not counted)
+        for (; i + kRoundUnroll <= i1; i += kRoundUnroll) {
+          PrimeRec pr[kRoundUnroll];
+          u32 xo[kRoundUnroll];
+          u64 hm[kRoundUnroll];
+#pragma unroll
+          for (int k = 0; k < kRoundUnroll; ++k) {
+            pr[k] = e.recs[i + k];
+            xo[k] = __ldg(xq + i + k);
+            hm[k] = KIND == KIND_DICKSON ? __ldg(e.hmask + i + k) : 0ull;
+          }
+          u32 kill = 0;
+#pragma unroll
+          for (int k = 0; k < kRoundUnroll; ++k) {
+            u32 rr = fk_bmod(v, pr[k].q, pr[k].magic) + xo[k];
+            rr = min(rr, rr - pr[k].q);
+            if (kill_test<KIND>(pr[k], rr, e.lists, S.sbits, e.xxmax, e.n,
+                                hm[k]))
+              kill |= 1u << k;
+          }
+          if (kill) {
+            i += __ffs((int)kill) - 1;
+            alive = false;
+            break;
+          }
+        }
+        for (; alive && i < i1; ++i) {
           const PrimeRec pr = e.recs[i];
           u32 rr = fk_bmod(v, pr.q, pr.magic) + __ldg(xq + i);
           rr = min(rr, rr - pr.q);
-          if (kill_test<KIND>(pr, rr, e.lists, S.sbits, e.xxmax, e.n)) {
+          const u64 hm = KIND == KIND_DICKSON ? __ldg(e.hmask + i) : 0ull;
+          if (kill_test<KIND>(pr, rr, e.lists, S.sbits, e.xxmax, e.n, hm)) {
             alive = false;
             break;
           }

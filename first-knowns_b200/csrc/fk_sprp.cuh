@@ -8,20 +8,10 @@
 // reference's on every input; above 3.317e24 they are strong-probable-
 // prime verdicts, exactly as the reference's are.
 //
-// Arithmetic is Montgomery's (Montgomery 1985): one 64-bit word for
-// m < 2^62, else CIOS (Koc, Acar, Kaliski 1996) over three to six 32-bit
-// limbs with PTX carry chains (fk_mont32.cuh).  The word count is chosen
-// so that 4m < R, which lets every residue stay in [0, 2m) between
-// products (lazy reduction: no conditional subtraction per product,
-// Walter's bound); residues are made canonical only to be compared.
-// -m^-1 mod 2^w comes by Newton iteration, R mod m by modular doubling
-// from 2^(bits-1), and a*R mod m for a base a by double-and-add.
-//
-// The exponent d of m - 1 = d * 2^s is read in bit pairs aligned to even
-// positions (they never straddle a 32-bit word): two squarings per pair,
-// then one product by a, a^2 or a^3 (precomputed) -- or, for base 2, up
-// to three modular doublings -- so lanes testing different bases of
-// same-sized values share the squarings and the loop shape.
+// Multiplication is CIOS Montgomery (Koc, Acar, Kaliski 1996) over
+// 32-bit limbs with PTX carry chains (fk_mont32.cuh), two to six limbs by
+// the value's size; reduction constants are -m^-1 mod 2^32 by Newton
+// iteration and R mod m, R^2 mod m by modular doubling.
 #pragma once
 #include "fk_arith.cuh"
 #include "fk_mont32.cuh"
@@ -91,155 +81,250 @@ __device__ __forceinline__ V3 v3_mul_128(u128 a, u128 b, bool* overflow) {
   return r;
 }
 
-// ---- trial division (huntlib/primes.py:31-33) ---------------------------
+// ---- Montgomery arithmetic on 64-bit limbs (one-limb values) -----------
 
-// Divisibility of a residue r < 2^32 by an odd prime p, by multiplying
-// with pinv = p^-1 mod 2^32 (Granlund and Montgomery 1994): p | r iff
-// r * pinv mod 2^32 <= lim = (2^32 - 1) / p.
-__device__ __forceinline__ bool divides(u32 r, u32 pinv, u32 lim) {
-  return r * pinv <= lim;
+template <int L>
+__device__ __forceinline__ int bitlen64(const u64* m) {
+  return 64 * (L - 1) + (64 - __clzll(m[L - 1]));
 }
 
-// x mod s for a value of three 64-bit limbs, c = 2^64 mod s, s < 2^28.
-__device__ __forceinline__ u32 mod3(const V3& v, u64 s, u64 c) {
-  u64 r = v.w[2] % s;
-  r = (r * c + v.w[1] % s) % s;
-  r = (r * c + v.w[0] % s) % s;
+// x = 2x mod m for x < m.
+template <int L>
+__device__ __forceinline__ void mdbl64(u64* x, const u64* m) {
+  u64 y[L];
+  u64 top = x[L - 1] >> 63;
+#pragma unroll
+  for (int i = L - 1; i > 0; --i) y[i] = (x[i] << 1) | (x[i - 1] >> 63);
+  y[0] = x[0] << 1;
+  // y (+ top * 2^(64L)) >= m ?
+  u64 d[L];
+  u64 br = 0;
+#pragma unroll
+  for (int i = 0; i < L; ++i) {
+    u64 t = y[i] - m[i];
+    u64 b1 = y[i] < m[i];
+    u64 t2 = t - br;
+    u64 b2 = t < br;
+    d[i] = t2;
+    br = b1 | b2;
+  }
+  bool ge = top || !br;
+#pragma unroll
+  for (int i = 0; i < L; ++i) x[i] = ge ? d[i] : y[i];
+}
+
+// r = a * b * 2^(-64L) mod m for a, b < m, m odd.  CIOS.
+template <int L>
+__device__ __forceinline__ void mmul64(u64* r, const u64* a, const u64* b,
+                                         const u64* m, u64 minv) {
+  u64 t[L + 2];
+#pragma unroll
+  for (int i = 0; i < L + 2; ++i) t[i] = 0;
+#pragma unroll
+  for (int i = 0; i < L; ++i) {
+    u64 c = 0;
+#pragma unroll
+    for (int j = 0; j < L; ++j) {
+      u128 p = (u128)a[j] * b[i] + t[j] + c;
+      t[j] = (u64)p;
+      c = (u64)(p >> 64);
+    }
+    u128 s = (u128)t[L] + c;
+    t[L] = (u64)s;
+    t[L + 1] = (u64)(s >> 64);
+    u64 q = t[0] * minv;
+    u128 p = (u128)q * m[0] + t[0];
+    c = (u64)(p >> 64);
+#pragma unroll
+    for (int j = 1; j < L; ++j) {
+      p = (u128)q * m[j] + t[j] + c;
+      t[j - 1] = (u64)p;
+      c = (u64)(p >> 64);
+    }
+    s = (u128)t[L] + c;
+    t[L - 1] = (u64)s;
+    t[L] = t[L + 1] + (u64)(s >> 64);
+  }
+  u64 d[L];
+  u64 br = 0;
+#pragma unroll
+  for (int i = 0; i < L; ++i) {
+    u64 x = t[i] - m[i];
+    u64 b1 = t[i] < m[i];
+    u64 x2 = x - br;
+    u64 b2 = x < br;
+    d[i] = x2;
+    br = b1 | b2;
+  }
+  bool ge = t[L] || !br;
+#pragma unroll
+  for (int i = 0; i < L; ++i) r[i] = ge ? d[i] : t[i];
+}
+
+template <int L>
+__device__ __forceinline__ bool eq64(const u64* a, const u64* b) {
+  bool e = true;
+#pragma unroll
+  for (int i = 0; i < L; ++i) e &= (a[i] == b[i]);
+  return e;
+}
+
+// Residue of the multi-limb m modulo a small modulus s (s < 2^31), from
+// the limbs top down with c = 2^64 mod s.
+template <int L>
+__device__ __forceinline__ u32 small_mod64(const u64* m, u32 s, u32 c) {
+  u64 r = 0;
+#pragma unroll
+  for (int i = L - 1; i >= 0; --i) r = (r * c + (m[i] % s)) % s;
   return (u32)r;
 }
 
-// Trial division of huntlib/primes.py:31-33 by the primes 2..37: 0 when m
-// is divisible by one of them and is not that prime (composite), 1 when m
-// is one of them (prime), 2 when none divides m (the strong tests decide).
-// Residues modulo 223092870 = 2*3*...*23 and 33263 = 29*31*37 carry it.
-__device__ __forceinline__ int sprp_trial(const V3& v) {
-  const bool small = (v.w[1] | v.w[2]) == 0;
-  if (small && v.w[0] < 2) return 0;
-  u32 r1, r2;
-  if (small) {
-    r1 = (u32)(v.w[0] % 223092870ull);
-    r2 = (u32)(v.w[0] % 33263ull);
-  } else {
-    r1 = mod3(v, 223092870ull, (~0ull % 223092870ull + 1) % 223092870ull);
-    r2 = mod3(v, 33263ull, (~0ull % 33263ull + 1) % 33263ull);
-  }
-  const u64 m = v.w[0];
-  if ((r1 & 1u) == 0) return (small && m == 2) ? 1 : 0;
-  // the odd primes to 23 and their inverses mod 2^32, then 29, 31, 37
-  constexpr u32 P1[8] = {3, 5, 7, 11, 13, 17, 19, 23};
-  constexpr u32 I1[8] = {0xAAAAAAABu, 0xCCCCCCCDu, 0xB6DB6DB7u, 0xBA2E8BA3u,
-                         0xC4EC4EC5u, 0xF0F0F0F1u, 0x286BCA1Bu, 0xE9BD37A7u};
-  constexpr u32 P2[3] = {29, 31, 37};
-  constexpr u32 I2[3] = {0x4F72C235u, 0xBDEF7BDFu, 0x914C1BADu};
+// Trial division of huntlib/primes.py:31-33 by the primes 2..37:
+// returns 0 (composite: divisible by a small prime it is not), 1 (m is one
+// of those primes, prime), or 2 (no small factor: go on).  Uses two
+// composite moduli, 223092870 = 2*3*5*7*11*13*17*19*23 and 33263 = 29*31*37.
+template <int L>
+__device__ __forceinline__ int trial64(const u64* m) {
+  if (L == 1 && m[0] < 2) return 0;
+  const u32 r1 = small_mod64<L>(
+      m, 223092870u, (u32)((18446744073709551615ull % 223092870ull + 1) % 223092870ull));
+  const u32 r2 = small_mod64<L>(
+      m, 33263u, (u32)((18446744073709551615ull % 33263ull + 1) % 33263ull));
+  const u32 sp1[9] = {2, 3, 5, 7, 11, 13, 17, 19, 23};
+  const u32 sp2[3] = {29, 31, 37};
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
-    if (divides(r1, I1[i], 0xFFFFFFFFu / P1[i]))
-      return (small && m == P1[i]) ? 1 : 0;
+  for (int i = 0; i < 9; ++i)
+    if (r1 % sp1[i] == 0) return (L == 1 && m[0] == sp1[i]) ? 1 : 0;
 #pragma unroll
   for (int i = 0; i < 3; ++i)
-    if (divides(r2, I2[i], 0xFFFFFFFFu / P2[i]))
-      return (small && m == P2[i]) ? 1 : 0;
+    if (r2 % sp2[i] == 0) return (L == 1 && m[0] == sp2[i]) ? 1 : 0;
   return 2;
 }
 
-// Algorithmic 32-bit multiply-adds of one strong test (CIOS on 32-bit
-// limbs): (bits - 1) squarings of 2l^2 + l word products, lo and hi each,
-// l = ceil(bits / 32) -- whatever representation the test actually uses.
-__device__ __forceinline__ u64 imad_alg(int bl) {
-  const u64 l = (u64)((bl + 31) >> 5);
-  return (u64)(bl - 1) * (4 * l * l + 2 * l);
-}
-
-// ---- one 64-bit word: m odd, 37 < m < 2^62, R = 2^64 ---------------------
-
-struct M64 {
-  u64 m, m2, minv;
+// Montgomery context over 64-bit limbs (used for one-limb values, where
+// one 64 x 64-bit product beats two 32-bit CIOS rounds).
+template <int L>
+struct Ctx64 {
+  u64 m[L], one[L], mone[L], d[L];
+  u64 minv;
+  int bl, s, dtop;
 };
 
-// a * b / R mod m in [0, 2m) for a, b < 2m: the low word of a*b + q*m is
-// zero by the choice of q, so only its carry (lo != 0) is needed.
-__device__ __forceinline__ u64 mul64(const M64& c, u64 a, u64 b) {
-  const u64 lo = a * b;
-  const u64 hi = __umul64hi(a, b);
-  const u64 q = lo * c.minv;
-  return hi + __umul64hi(q, c.m) + (lo != 0 ? 1ull : 0ull);
-}
-
-__device__ __forceinline__ u64 dbl64(const M64& c, u64 x) {  // [0, 2m)
-  const u64 y = x << 1;
-  return y >= c.m2 ? y - c.m2 : y;
-}
-
-__device__ __forceinline__ bool strong64(u64 m, u32 a, u64* imad) {
-  M64 c;
-  c.m = m;
-  c.m2 = m << 1;
-  u64 inv = m;  // m * m == 1 mod 8: correct to 3 bits, doubling each step
+template <int L>
+__device__ __forceinline__ void ctx_init64(Ctx64<L>& c, const u64* m) {
 #pragma unroll
-  for (int i = 0; i < 5; ++i) inv *= 2 - m * inv;
-  c.minv = 0 - inv;
-  const int bl = 64 - __clzll((long long)m);
-  u64 one = 1ull << (bl - 1);  // < m, doubled to 2^64 mod m
-  for (int i = 0; i < 64 - bl + 1; ++i) {
-    one <<= 1;
-    one = one >= m ? one - m : one;
+  for (int i = 0; i < L; ++i) c.m[i] = m[i];
+  u64 minv = m[0];  // m * m == 1 mod 8: correct to 3 bits
+#pragma unroll
+  for (int i = 0; i < 5; ++i) minv *= 2 - m[0] * minv;
+  c.minv = (u64)0 - minv;  // -m^-1 mod 2^64
+  c.bl = bitlen64<L>(m);
+#pragma unroll
+  for (int i = 0; i < L; ++i) c.one[i] = 0;
+  c.one[(c.bl - 1) >> 6] = 1ull << ((c.bl - 1) & 63);  // 2^(bl-1) < m
+  for (int i = 0; i < 64 * L - c.bl + 1; ++i) mdbl64<L>(c.one, m);
+  u64 br = 0;
+#pragma unroll
+  for (int i = 0; i < L; ++i) {  // m - (R mod m): -1 in Montgomery form
+    const u64 x = m[i] - c.one[i];
+    const u64 b1 = m[i] < c.one[i];
+    const u64 x2 = x - br;
+    const u64 b2 = x < br;
+    c.mone[i] = x2;
+    br = b1 | b2;
   }
-  const u64 dm = m - 1;
-  const int s = __ffsll((long long)dm) - 1;
-  const u64 d = dm >> s;
-  const int dtop = 63 - __clzll((long long)d);
-  *imad += imad_alg(bl);
-  const bool b2 = a == 2;
-  if (m <= a) {  // huntlib: a %= m, a zero base is skipped
-    a = (u32)(a % m);
-    if (a == 0) return true;
+#pragma unroll
+  for (int i = 0; i < L; ++i) c.d[i] = m[i];
+  c.d[0] -= 1;  // m odd
+  int lz = 0;
+  while (c.d[lz] == 0) ++lz;
+  c.s = 64 * lz + __ffsll((long long)c.d[lz]) - 1;
+  const int ws = c.s >> 6, bs = c.s & 63;
+#pragma unroll
+  for (int i = 0; i < L; ++i) {
+    const u64 lo = (i + ws < L) ? c.d[i + ws] : 0;
+    const u64 hi = (i + ws + 1 < L) ? c.d[i + ws + 1] : 0;
+    c.d[i] = bs ? ((lo >> bs) | (hi << (64 - bs))) : lo;
   }
-  u64 t1 = one, t2 = one, t3 = one;
-  if (!b2) {  // a * R mod m by double-and-add, then a^2, a^3
-    u64 r = one;
-    for (int b = 30 - __clz(a); b >= 0; --b) {
-      r <<= 1;
-      r = r >= m ? r - m : r;
-      if ((a >> b) & 1u) {
-        r += one;
-        r = r >= m ? r - m : r;
-      }
-    }
-    t1 = r;
-    t2 = mul64(c, t1, t1);
-    t3 = mul64(c, t2, t1);
-  }
-  int b = dtop | 1;  // the aligned pair (b, b - 1) holding the top bit
-  u32 w = (u32)(d >> (b - 1)) & 3u;
-  u64 x;
-  if (b2) {
-    x = one;
-    for (u32 k = 0; k < w; ++k) x = dbl64(c, x);
-  } else {
-    x = w == 1 ? t1 : (w == 2 ? t2 : t3);
-  }
-  for (b -= 2; b >= 1; b -= 2) {
-    x = mul64(c, x, x);
-    x = mul64(c, x, x);
-    w = (u32)(d >> (b - 1)) & 3u;
-    if (b2) {
-      for (u32 k = 0; k < w; ++k) x = dbl64(c, x);
-    } else if (w) {
-      x = mul64(c, x, w == 1 ? t1 : (w == 2 ? t2 : t3));
-    }
-  }
-  const u64 mone = m - one;
-  x = x >= m ? x - m : x;
-  if (x == one || x == mone) return true;
-  for (int r = 1; r < s; ++r) {
-    x = mul64(c, x, x);
-    x = x >= m ? x - m : x;
-    if (x == mone) return true;
+  c.dtop = 0;
+#pragma unroll
+  for (int i = L - 1; i >= 0; --i)
+    if (c.d[i] && c.dtop == 0) c.dtop = 64 * i + 63 - __clzll(c.d[i]);
+}
+
+// Algorithmic 32-bit multiply-adds of one strong test (CIOS on 32-bit
+// limbs): (bits - 1) squarings of 2l^2 + l word products, lo and hi each.
+template <int L>
+__device__ __forceinline__ u64 imad64(const Ctx64<L>& c) {
+  const u64 l32 = (u64)((c.bl + 31) >> 5);
+  return (u64)(c.bl - 1) * (4 * l32 * l32 + 2 * l32);
+}
+
+// The strong-test tail: x = a^d already in Montgomery form.
+template <int L>
+__device__ __forceinline__ bool tail64(const Ctx64<L>& c, u64* x) {
+  if (eq64<L>(x, c.one) || eq64<L>(x, c.mone)) return true;
+  for (int r = 1; r < c.s; ++r) {
+    mmul64<L>(x, x, x, c.m, c.minv);
+    if (eq64<L>(x, c.mone)) return true;
   }
   return false;
 }
 
-// ---- N 32-bit words (N = 3..6): m odd, 4m < 2^(32N) ----------------------
+// One strong test of m to base kMrBases[bi] (bi = 0 is base 2), with the
+// trial division first: the unit of work of the step interpreter in
+// k_classify.  Every base runs the same loop shape -- square, then on a set
+// bit of d multiply by the base (a modular doubling for base 2) -- so lanes
+// testing different bases of same-sized values stay converged.
+template <int L>
+__device__ __forceinline__ bool step64(const u64* m, int bi, u64* imad) {
+  const int t = trial64<L>(m);
+  if (t != 2) return t == 1;
+  Ctx64<L> c;
+  ctx_init64<L>(c, m);
+  u64 at[L];
+  bool is2 = bi == 0;
+  if (!is2) {
+    u64 a = kMrBases[bi];
+    if (L == 1 && c.m[0] <= a) {
+      a %= c.m[0];
+      if (a == 0) return true;  // huntlib skips a zero base
+    }
+    u64 r2m[L], av[L];
+#pragma unroll
+    for (int i = 0; i < L; ++i) { r2m[i] = c.one[i]; av[i] = 0; }
+    for (int i = 0; i < 64 * L; ++i) mdbl64<L>(r2m, c.m);
+    av[0] = a;
+    mmul64<L>(at, av, r2m, c.m, c.minv);  // a * R mod m
+  }
+  *imad += imad64<L>(c);
+  u64 x[L];
+#pragma unroll
+  for (int i = 0; i < L; ++i) x[i] = c.one[i];
+  for (int b = c.dtop; b >= 0; --b) {
+    mmul64<L>(x, x, x, c.m, c.minv);
+    if ((c.d[b >> 6] >> (b & 63)) & 1) {
+      if (is2) mdbl64<L>(x, c.m);
+      else mmul64<L>(x, x, at, c.m, c.minv);
+    }
+  }
+  return tail64<L>(c, x);
+}
+
+
+// ---- Montgomery arithmetic on N 32-bit limbs (N = 2..6) -----------------
+// A value below 2^(32N) as N little-endian 32-bit words.  Products use the
+// carry-chained multiply-accumulate pass of fk_mont32.cuh, so one word
+// product is one mad.lo and one mad.hi -- the two IMADs per product the
+// algorithmic count charges.
+
+template <int N>
+__device__ __forceinline__ int bitlen32(const u32* m) {
+#pragma unroll
+  for (int i = N - 1; i > 0; --i)
+    if (m[i]) return 32 * i + 32 - __clz(m[i]);
+  return 32 - __clz(m[0]);
+}
 
 // d = x - y over N words; returns the borrow out.
 template <int N>
@@ -254,41 +339,24 @@ __device__ __forceinline__ u32 sub_n(u32* d, const u32* x, const u32* y) {
   return br;
 }
 
-// x = x - y when x >= y (in place).
+// x = 2x mod m for x < m.
 template <int N>
-__device__ __forceinline__ void csub_n(u32* x, const u32* y) {
-  u32 d[N];
-  const u32 br = sub_n<N>(d, x, y);
-#pragma unroll
-  for (int i = 0; i < N; ++i) x[i] = br ? x[i] : d[i];
-}
-
-// x = x - m when `carry` (a bit above the N words) is set or x >= m.
-template <int N>
-__device__ __forceinline__ void csub_c(u32* x, u32 carry, const u32* m) {
-  u32 d[N];
-  const u32 br = sub_n<N>(d, x, m);
-  const bool ge = carry || !br;
-#pragma unroll
-  for (int i = 0; i < N; ++i) x[i] = ge ? d[i] : x[i];
-}
-
-// x = 2x mod m for x < m (the bit shifted out of the top word counts).
-template <int N>
-__device__ __forceinline__ void dbl_n(u32* x, const u32* m) {
+__device__ __forceinline__ void mdbl32(u32* x, const u32* m) {
+  u32 y[N], d[N];
   const u32 top = x[N - 1] >> 31;
 #pragma unroll
-  for (int i = N - 1; i > 0; --i) x[i] = (x[i] << 1) | (x[i - 1] >> 31);
-  x[0] <<= 1;
-  csub_c<N>(x, top, m);
+  for (int i = N - 1; i > 0; --i) y[i] = (x[i] << 1) | (x[i - 1] >> 31);
+  y[0] = x[0] << 1;
+  const u32 br = sub_n<N>(d, y, m);
+  const bool ge = top || !br;
+#pragma unroll
+  for (int i = 0; i < N; ++i) x[i] = ge ? d[i] : y[i];
 }
 
-// r = a * b / R mod m for R = 2^(32N), by CIOS.  Lazy (4m < R): a, b < 2m
-// give r < 2m with no final subtraction (the top word stays zero).
-// Strict: a, b < m give r < m after one conditional subtraction.
-template <int N, bool Strict = false>
-__device__ __forceinline__ void mul_n(u32* r, const u32* a, const u32* b,
-                                      const u32* m, u32 minv) {
+// r = a * b * 2^(-32N) mod m for a, b < m, m odd (CIOS; r may alias a/b).
+template <int N>
+__device__ __forceinline__ void mmul32(u32* r, const u32* a, const u32* b,
+                                       const u32* m, u32 minv) {
   u32 t[N + 2];
 #pragma unroll
   for (int i = 0; i < N + 2; ++i) t[i] = 0;
@@ -296,199 +364,207 @@ __device__ __forceinline__ void mul_n(u32* r, const u32* a, const u32* b,
   for (int i = 0; i < N; ++i) {
     Mont32<N>::mac(t, a, b[i]);
     const u32 q = t[0] * minv;
-    Mont32<N>::mac(t, m, q);  // t[0] becomes 0
+    Mont32<N>::mac(t, m, q);       // t[0] becomes 0
 #pragma unroll
     for (int j = 0; j < N + 1; ++j) t[j] = t[j + 1];
     t[N + 1] = 0;
   }
-  if (Strict) csub_c<N>(t, t[N], m);
+  u32 d[N];
+  const u32 br = sub_n<N>(d, t, m);
+  const bool ge = t[N] || !br;
 #pragma unroll
-  for (int i = 0; i < N; ++i) r[i] = t[i];
+  for (int i = 0; i < N; ++i) r[i] = ge ? d[i] : t[i];
 }
 
 template <int N>
-__device__ __forceinline__ bool eq_n(const u32* a, const u32* b) {
+__device__ __forceinline__ bool eq32(const u32* a, const u32* b) {
   bool e = true;
 #pragma unroll
   for (int i = 0; i < N; ++i) e &= (a[i] == b[i]);
   return e;
 }
 
+// Residue of m modulo a small modulus s (s < 2^31), from the top word
+// down with c = 2^32 mod s.
 template <int N>
-__device__ __forceinline__ void sel_n(u32* r, u32 w, const u32* t1,
-                                      const u32* t2, const u32* t3) {
+__device__ __forceinline__ u32 small_mod32(const u32* m, u32 s, u32 c) {
+  u64 r = 0;
 #pragma unroll
-  for (int i = 0; i < N; ++i) r[i] = w == 1 ? t1[i] : (w == 2 ? t2[i] : t3[i]);
+  for (int i = N - 1; i >= 0; --i) r = (r * c + m[i] % s) % s;
+  return (u32)r;
 }
 
-// One strong test on N words.  Lazy residues need 4m < R (bits <= 32N -
-// 2); Strict keeps every residue canonical and serves the 191- and 192-bit
-// values that six words hold without that margin.
-template <int N, bool Strict = false>
-__device__ __forceinline__ bool strong_n(const u32* m, u32 a, u64* imad) {
-  u32 inv = m[0];
+// Trial division of huntlib/primes.py:31-33 by the primes 2..37:
+// returns 0 (composite: divisible by a small prime it is not), 1 (m is one
+// of those primes, prime), or 2 (no small factor: go on).  Uses two
+// composite moduli, 223092870 = 2*3*5*7*11*13*17*19*23 and 33263 = 29*31*37.
+template <int N>
+__device__ __forceinline__ int trial_small(const u32* m) {
+  bool small = true;
+#pragma unroll
+  for (int i = 1; i < N; ++i) small &= (m[i] == 0);
+  if (small && m[0] < 2) return 0;
+  const u32 r1 = small_mod32<N>(m, 223092870u,
+                                (u32)((1ull << 32) % 223092870ull));
+  const u32 r2 = small_mod32<N>(m, 33263u, (u32)((1ull << 32) % 33263ull));
+  const u32 sp1[9] = {2, 3, 5, 7, 11, 13, 17, 19, 23};
+  const u32 sp2[3] = {29, 31, 37};
+#pragma unroll
+  for (int i = 0; i < 9; ++i)
+    if (r1 % sp1[i] == 0) return (small && m[0] == sp1[i]) ? 1 : 0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    if (r2 % sp2[i] == 0) return (small && m[0] == sp2[i]) ? 1 : 0;
+  return 2;
+}
+
+// Montgomery context of an odd m > 37 with no small factor: R = 2^(32N).
+template <int N>
+struct Ctx {
+  u32 m[N], one[N], mone[N], d[N];
+  u32 minv;
+  int bl, s, dtop;
+};
+
+template <int N>
+__device__ __forceinline__ void ctx_init(Ctx<N>& c, const u32* m) {
+#pragma unroll
+  for (int i = 0; i < N; ++i) c.m[i] = m[i];
+  u32 inv = m[0];  // m * m == 1 mod 8: correct to 3 bits
 #pragma unroll
   for (int i = 0; i < 4; ++i) inv *= 2u - m[0] * inv;
-  const u32 minv = 0u - inv;
-  int bl = 0;
+  c.minv = 0u - inv;  // -m^-1 mod 2^32
+  c.bl = bitlen32<N>(m);
 #pragma unroll
-  for (int i = 0; i < N; ++i)
-    if (m[i]) bl = 32 * i + 32 - __clz(m[i]);
-  *imad += imad_alg(bl);
-  // R mod m: 2^(bl - 1) doubled 32N - bl + 1 times, canonical
-  u32 one[N];
+  for (int i = 0; i < N; ++i) c.one[i] = 0;
+  c.one[(c.bl - 1) >> 5] = 1u << ((c.bl - 1) & 31);  // 2^(bl-1) < m
+  for (int i = 0; i < 32 * N - c.bl + 1; ++i) mdbl32<N>(c.one, m);
+  sub_n<N>(c.mone, m, c.one);  // -1 in Montgomery form
 #pragma unroll
-  for (int i = 0; i < N; ++i)
-    one[i] = ((bl - 1) >> 5) == i ? 1u << ((bl - 1) & 31) : 0u;
-  for (int i = 0; i < 32 * N - bl + 1; ++i) dbl_n<N>(one, m);
-  // m - 1 = d * 2^s
-  u32 d[N];
+  for (int i = 0; i < N; ++i) c.d[i] = m[i];
+  c.d[0] -= 1;  // m odd
+  int lz = 0;
+  while (c.d[lz] == 0) ++lz;
+  c.s = 32 * lz + __ffs((int)c.d[lz]) - 1;
+  const int ws = c.s >> 5, bs = c.s & 31;
 #pragma unroll
-  for (int i = 0; i < N; ++i) d[i] = m[i];
-  d[0] -= 1;  // m odd: no borrow
-  int s = 0;
-  while (d[0] == 0) {  // whole zero words: shift down (indices stay static)
-#pragma unroll
-    for (int i = 0; i < N - 1; ++i) d[i] = d[i + 1];
-    d[N - 1] = 0;
-    s += 32;
+  for (int i = 0; i < N; ++i) {
+    const u32 lo = (i + ws < N) ? c.d[i + ws] : 0;
+    const u32 hi = (i + ws + 1 < N) ? c.d[i + ws + 1] : 0;
+    c.d[i] = bs ? ((lo >> bs) | (hi << (32 - bs))) : lo;
   }
-  const int bs = __ffs((int)d[0]) - 1;
-  s += bs;
-  if (bs) {
+  c.dtop = 0;
 #pragma unroll
-    for (int i = 0; i < N - 1; ++i) d[i] = (d[i] >> bs) | (d[i + 1] << (32 - bs));
-    d[N - 1] >>= bs;
-  }
-  int dtop = 0;
-#pragma unroll
-  for (int i = 0; i < N; ++i)
-    if (d[i]) dtop = 32 * i + 31 - __clz(d[i]);
-  const bool b2 = a == 2;
-  u32 t1[N], t2[N], t3[N];
-  if (!b2) {  // a * R mod m by double-and-add (a < 2^31 < m), then a^2, a^3
-#pragma unroll
-    for (int i = 0; i < N; ++i) t1[i] = one[i];
-    for (int b = 30 - __clz(a); b >= 0; --b) {
-      dbl_n<N>(t1, m);
-      if ((a >> b) & 1u) {
-        u32 c = 0;
-#pragma unroll
-        for (int i = 0; i < N; ++i) {
-          const u64 x = (u64)t1[i] + one[i] + c;
-          t1[i] = (u32)x;
-          c = (u32)(x >> 32);
-        }
-        csub_c<N>(t1, c, m);
-      }
-    }
-    mul_n<N, Strict>(t2, t1, t1, m, minv);
-    mul_n<N, Strict>(t3, t2, t1, m, minv);
-  }
-  // the aligned bit pairs of d, top down; pairs never straddle a word
-  u32 x[N];
-  bool started = false;
-#pragma unroll
-  for (int wi = N - 1; wi >= 0; --wi) {
-    if (32 * wi > dtop) continue;
-    const u32 dw = d[wi];
-    const int top = (32 * wi + 31 > dtop) ? (dtop & 31) : 31;
-    for (int b = top | 1; b >= 1; b -= 2) {
-      const u32 w = (dw >> (b - 1)) & 3u;
-      if (started) {
-        mul_n<N, Strict>(x, x, x, m, minv);
-        mul_n<N, Strict>(x, x, x, m, minv);
-        if (b2) {  // canonical first, then doublings mod m stay below m
-          if (w) csub_n<N>(x, m);
-          for (u32 k = 0; k < w; ++k) dbl_n<N>(x, m);
-        } else if (w) {
-          u32 y[N];
-          sel_n<N>(y, w, t1, t2, t3);
-          mul_n<N, Strict>(x, x, y, m, minv);
-        }
-      } else {
-        started = true;
-        if (b2) {
-#pragma unroll
-          for (int i = 0; i < N; ++i) x[i] = one[i];
-          for (u32 k = 0; k < w; ++k) dbl_n<N>(x, m);
-        } else {
-          sel_n<N>(x, w, t1, t2, t3);
-        }
-      }
-    }
-  }
-  u32 mone[N];
-  sub_n<N>(mone, m, one);
-  csub_n<N>(x, m);
-  if (eq_n<N>(x, one) || eq_n<N>(x, mone)) return true;
-  for (int r = 1; r < s; ++r) {
-    mul_n<N, Strict>(x, x, x, m, minv);
-    csub_n<N>(x, m);
-    if (eq_n<N>(x, mone)) return true;
+  for (int i = N - 1; i >= 0; --i)
+    if (c.d[i] && c.dtop == 0) c.dtop = 32 * i + 31 - __clz(c.d[i]);
+}
+
+// Algorithmic 32-bit multiply-adds of one strong test (CIOS on 32-bit
+// limbs): (bits - 1) squarings of 2l^2 + l word products, lo and hi each.
+template <int N>
+__device__ __forceinline__ u64 imad_per_base(const Ctx<N>& c) {
+  const u64 l32 = (u64)((c.bl + 31) >> 5);
+  return (u64)(c.bl - 1) * (4 * l32 * l32 + 2 * l32);
+}
+
+// The strong-test tail: x = a^d already in Montgomery form.
+template <int N>
+__device__ __forceinline__ bool strong_tail(const Ctx<N>& c, u32* x) {
+  if (eq32<N>(x, c.one) || eq32<N>(x, c.mone)) return true;
+  for (int r = 1; r < c.s; ++r) {
+    mmul32<N>(x, x, x, c.m, c.minv);
+    if (eq32<N>(x, c.mone)) return true;
   }
   return false;
 }
 
-// The strong test of a value of 2^62 or more (three 64-bit limbs) to base
-// a, on N = ceil((bits + 2) / 32) 32-bit words, which keeps 4m < R, or on
-// six words with canonical residues for 191 and 192 bits.  Kept
-// out of line, with scalars in and out, so the common one-word path of the
-// callers keeps its registers: returns the algorithmic IMADs << 1 | pass.
-__device__ __noinline__ u64 strong_wide(u64 w0, u64 w1, u64 w2, u32 a) {
-  u32 w[6] = {(u32)w0, (u32)(w0 >> 32), (u32)w1, (u32)(w1 >> 32), (u32)w2,
-              (u32)(w2 >> 32)};
-  int bl = 0;
-#pragma unroll
-  for (int i = 0; i < 6; ++i)
-    if (w[i]) bl = 32 * i + 32 - __clz(w[i]);
-  const int n = (bl + 2 + 31) >> 5;
-  u64 im = 0;
-  bool pass;
-  if (n <= 3) pass = strong_n<3>(w, a, &im);
-  else if (n == 4) pass = strong_n<4>(w, a, &im);
-  else if (n == 5) pass = strong_n<5>(w, a, &im);
-  else if (n == 6) pass = strong_n<6>(w, a, &im);
-  else pass = strong_n<6, true>(w, a, &im);
-  return (im << 1) | (pass ? 1ull : 0ull);
-}
-
-// One strong test of v to base kMrBases[bi] (bi = 0 is base 2), for a v
-// that trial division left undecided (odd, above 37, no factor <= 37).
-// Values below 2^62 take one 64-bit word, larger ones strong_wide.
-__device__ __forceinline__ bool sprp_strong(const V3& v, int bi, u64* imad) {
-  const u32 a = kMrBases[bi];
-  if (v.w[1] == 0 && v.w[2] == 0 && v.w[0] < (1ull << 62))
-    return strong64(v.w[0], a, imad);
-  const u64 r = strong_wide(v.w[0], v.w[1], v.w[2], a);
-  *imad += r >> 1;
-  return (r & 1) != 0;
-}
-
-// One base of huntlib's test: the trial division, then the strong test.
-__device__ __forceinline__ bool sprp_step(const V3& v, int bi, u64* imad) {
-  const int t = sprp_trial(v);
+// One strong test of m to base kMrBases[bi] (bi = 0 is base 2), with the
+// trial division first.  Every base runs the same loop shape -- square,
+// then on a set bit of d multiply by the base (a modular doubling for base
+// 2, so base 2 needs no R^2) -- so lanes testing different bases of
+// same-sized values stay converged.
+template <int N>
+__device__ __forceinline__ bool step_N(const u32* m, int bi, u64* imad) {
+  const int t = trial_small<N>(m);
   if (t != 2) return t == 1;
-  return sprp_strong(v, bi, imad);
+  Ctx<N> c;
+  ctx_init<N>(c, m);
+  u32 at[N];
+  const bool is2 = bi == 0;
+  if (!is2) {
+    u32 a = kMrBases[bi];
+    bool small = true;
+#pragma unroll
+    for (int i = 1; i < N; ++i) small &= (c.m[i] == 0);
+    if (small && c.m[0] <= a) {
+      a %= c.m[0];
+      if (a == 0) return true;  // huntlib skips a zero base
+    }
+    u32 r2m[N], av[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) { r2m[i] = c.one[i]; av[i] = 0; }
+    for (int i = 0; i < 32 * N; ++i) mdbl32<N>(r2m, c.m);  // R^2 mod m
+    av[0] = a;
+    mmul32<N>(at, av, r2m, c.m, c.minv);  // a * R mod m
+  }
+  *imad += imad_per_base<N>(c);
+  u32 x[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) x[i] = c.one[i];
+  u32 dw = 0;
+  for (int b = c.dtop; b >= 0; --b) {
+    if (b == c.dtop || (b & 31) == 31) dw = c.d[b >> 5];  // once a word
+    mmul32<N>(x, x, x, c.m, c.minv);
+    if ((dw >> (b & 31)) & 1u) {
+      if (is2) mdbl32<N>(x, c.m);
+      else mmul32<N>(x, x, at, c.m, c.minv);
+    }
+  }
+  return strong_tail<N>(c, x);
+}
+
+// The value's 32-bit words and the limb count it needs (at least 2).
+__device__ __forceinline__ int to_words(const V3& v, u32* w) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    w[2 * i] = (u32)v.w[i];
+    w[2 * i + 1] = (u32)(v.w[i] >> 32);
+  }
+  int n = 6;
+  while (n > 2 && w[n - 1] == 0) --n;
+  return n;
+}
+
+__device__ __noinline__ bool sprp_step(const V3& v, int bi, u64* imad) {
+  if (v.w[1] == 0 && v.w[2] == 0) return step64<1>(v.w, bi, imad);
+  u32 w[6];
+  switch (to_words(v, w)) {
+    case 6: return step_N<6>(w, bi, imad);
+    case 5: return step_N<5>(w, bi, imad);
+    case 4: return step_N<4>(w, bi, imad);
+    case 3: return step_N<3>(w, bi, imad);
+    default: return step_N<2>(w, bi, imad);
+  }
+}
+
+// which = 0: mr_is_prime, 1: sprp_base2, 2: the six bases after 2 only
+// (callers that already know m passes base 2).
+__device__ __noinline__ bool sprp_which(const V3& v, int which, u64* imad) {
+  if (which != 2 && !sprp_step(v, 0, imad)) return false;
+  if (which == 1) return true;
+  for (int bi = 1; bi < 7; ++bi)
+    if (!sprp_step(v, bi, imad)) return false;
+  return true;
 }
 
 // mr_is_prime (base2_only = false) or sprp_base2 (true).
 __device__ __forceinline__ bool sprp(const V3& v, bool base2_only, u64* imad) {
-  const int t = sprp_trial(v);
-  if (t != 2) return t == 1;
-  const int nb = base2_only ? 1 : 7;
-  for (int bi = 0; bi < nb; ++bi)
-    if (!sprp_strong(v, bi, imad)) return false;
-  return true;
+  return sprp_which(v, base2_only ? 1 : 0, imad);
 }
 
 // The six bases after 2 (v already passed base 2 and trial division).
 __device__ __forceinline__ bool sprp_rest(const V3& v, u64* imad) {
-  const int t = sprp_trial(v);
-  if (t != 2) return t == 1;
-  for (int bi = 1; bi < 7; ++bi)
-    if (!sprp_strong(v, bi, imad)) return false;
-  return true;
+  return sprp_which(v, 2, imad);
 }
 
 }  // namespace fk

@@ -53,6 +53,8 @@ struct DevEngine {
   const PrimeRec* recs;           // [NP]
   const uint32_t* c64;            // [NP] 2^64 mod q
   const uint32_t* lists;          // explicit forbidden-residue lists
+  const uint64_t* hmask;          // [NP] Dickson: bit (h mod 64) set for
+                                  // each half residue h on the prime's list
   const uint32_t* rounds;         // [nrounds + 1] prime-index cuts
   const uint32_t* sbits;          // Euler: bitset of {x^2 + x : x < n}
   // marking sieve (long lanes): primes [NS, NPm) are marked in a per-lane
