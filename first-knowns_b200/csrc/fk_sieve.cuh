@@ -102,10 +102,16 @@ __device__ __forceinline__ bool kill_test(const PrimeRec& pr, u32 r,
     // j = (q - r) * d^-1 mod q is below n; aux = d^-1 (0 when q | d).
     if (r == 0) return true;
     if (pr.aux == 0) return false;
-    // (q - r) * d^-1 < q^2 < 2^32: a 32-bit Barrett with floor(2^32 / q)
-    const u32 x = (pr.q - r) * pr.aux;
-    u32 t = x - __umulhi(x, (u32)(pr.magic >> 32)) * pr.q;
-    t = min(t, t - pr.q);
+    // for q < 2^16 the product (q - r) * d^-1 < q^2 fits 32 bits: a
+    // 32-bit Barrett with floor(2^32 / q); deeper primes take 64 bits
+    u32 t;
+    if (pr.q < 65536u) {
+      const u32 x = (pr.q - r) * pr.aux;
+      t = x - __umulhi(x, (u32)(pr.magic >> 32)) * pr.q;
+      t = min(t, t - pr.q);
+    } else {
+      t = fk_mulmod(pr.q - r, pr.aux, pr.q, pr.magic);
+    }
     return t < n;
   }
   return false;  // Dickson primes always carry a list
