@@ -460,7 +460,7 @@ static fk_status build_engine(fk_engine* e) {
   // cut into sub-ranges of at least kMarkHits hits and at most 8 per
   // segment, ordered by prime so a warp's entries share q and trip counts
   std::vector<u64> mq;
-  std::vector<u32> mitems;
+  std::vector<u64> mitems;
   for (u32 i = kNS; i < NPm; ++i) {
     const u32 q = e->sieve[i];
     const u32 pi = i - kNS;
@@ -475,7 +475,8 @@ static fk_status build_engine(fk_engine* e) {
     const u32 go = gaux[i] & 0x00FFFFFFu, gc = gaux[i] >> 24;
     for (u32 k = 0; k < nsub; ++k)
       for (u32 c = 0; c < gc; ++c)
-        mitems.push_back(glist[go + c] | (pi << 16) | (k << 29));
+        mitems.push_back((u64)(glist[go + c] | (pi << 16) | (k << 29)) |
+                         ((u64)q << 32) | ((u64)S << 48));
   }
   e->mprefix.push_back((u32)mitems.size());
   e->cost = engine_cost(e, NPm);

@@ -183,20 +183,20 @@ __global__ void __launch_bounds__(kBlock, 3) k_mark(SieveArgs a) {
       __syncthreads();
       // (b) mark: the work entries round robin over the threads, the next
       // entry's load in flight while this one's progression is written
+      // (an entry carries its prime and sub-range length: one load each)
       {
         const u32 nm = e.nmitems;
-        const u32* __restrict__ mit = e.mitems;
-        const u64* __restrict__ mqt = reinterpret_cast<const u64*>(e.mq);
+        const u64* __restrict__ mit = reinterpret_cast<const u64*>(e.mitems);
         unsigned char* __restrict__ B = S.bytes;
         u32 cnt = 0;
         u32 i = tid;
-        u32 w = i < nm ? __ldg(mit + i) : 0u;
+        u64 w = i < nm ? __ldg(mit + i) : 0ull;
         while (i < nm) {
           const u32 inext = i + kBlock;
-          const u32 wn = inext < nm ? __ldg(mit + inext) : 0u;
-          const u32 g = w & 0xFFFFu, pi = (w >> 16) & 0x1FFFu, k = w >> 29;
-          const u64 m = __ldg(mqt + pi);
-          const u32 q = (u32)m & 0xFFFFu, sl = (u32)(m >> 32);
+          const u64 wn = inext < nm ? __ldg(mit + inext) : 0ull;
+          const u32 wl = (u32)w, wh = (u32)(w >> 32);
+          const u32 g = wl & 0xFFFFu, pi = (wl >> 16) & 0x1FFFu, k = wl >> 29;
+          const u32 q = wh & 0xFFFFu, sl = wh >> 16;
           const u32 off = S.off16[pi];
           u32 h = (g >= off ? g - off : g + q - off) + k * sl;
           const u32 end = sl ? min(seg_len, (k + 1) * sl) : seg_len;

@@ -38,7 +38,7 @@
 namespace fk {
 
 constexpr u32 kWaitSpins = 1u << 20;
-constexpr int kRoundUnroll = 4;  // primes per trip of the compaction rounds
+constexpr int kRoundUnroll = 2;  // primes per trip of the compaction rounds
 
 __device__ __forceinline__ u32 smem_u32(const void* p) {
   return (u32)__cvta_generic_to_shared(p);

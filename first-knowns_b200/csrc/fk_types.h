@@ -69,9 +69,10 @@ struct DevEngine {
   // S is the length of one work entry's sub-range (a multiple of q; 0 when
   // one entry covers the whole segment)
   const uint64_t* mq;
-  // [nmitems] work entries g | (prime - NS) << 16 | sub-range << 29: the
-  // hits u = g (mod q), shifted by the lane, inside sub-range k
-  const uint32_t* mitems;
+  // [nmitems] work entries g | (prime - NS) << 16 | sub-range k << 29 |
+  // q << 32 | S << 48: the hits u = g (mod q), shifted by the lane, inside
+  // sub-range k of length S (one load per entry: q and S ride along)
+  const uint64_t* mitems;
 };
 
 // One unit of work: a sub-range of one engine's line.
