@@ -404,10 +404,14 @@ def reference_scores(runs=3):
 def serve_bench(args):
     """The served workload (Poisson arrivals; length 2^U(16,34), threshold
     6..14, start 10^U(18,24)) through the continuous-batching loop.  The
-    arrival rate is 80% of the loop's measured capacity (256 requests
-    queued at once and served back to back give requests/s at full load).
-    Reports p50/p99 latency overall and per length class, the device-time
-    fraction, and the same arrivals through a single slot (no overlap)."""
+    arrival rate is 60% of the loop's capacity measured with 256 requests
+    queued at once and served back to back (full batches: streaming
+    arrivals make smaller batches, whose fixed cost per batch lowers the
+    sustainable rate, so 80% of this figure already overloads the loop).
+    Reports p50/p99 latency overall and per length class, the fraction of
+    wall time with a batch in flight, the summed device time of all batches
+    over wall time (above 1 when the two slots overlap), and the same
+    arrivals through a single slot (no overlap)."""
     import numpy as np
     import fk_workloads as W
     from fk_serve import ServeLoop
@@ -417,7 +421,7 @@ def serve_bench(args):
     loop.run([(0.0, iv) for iv in sample[:32]])        # warm: tables, buffers
     _, _, cst = loop.run([(0.0, iv) for iv in sample])
     capacity = len(sample) / cst["wall_s"]
-    rate = 0.8 * capacity
+    rate = 0.6 * capacity
     reqs = W.served(count=int(rate * args.serve_seconds * 1.5) + 64,
                     rate_hz=rate)
     lens = np.array([iv.length for _, iv in reqs], dtype=float)
@@ -430,6 +434,7 @@ def serve_bench(args):
                "p99_ms": float(np.percentile(lat[done], 99) * 1e3),
                "throughput": float(lens[done].sum() / st["wall_s"]),
                "unit": UNIT, "batches": st["batches"],
+               "inflight_frac": st["inflight_s"] / st["wall_s"],
                "device_time_frac": st["device_busy_s"] / st["wall_s"]}
         classes = {}
         for name, lo, hi in (("short <2^22", 0, 2 ** 22),
@@ -448,11 +453,12 @@ def serve_bench(args):
     one = summary(ServeLoop(engset=loop.engset, slots=1),
                   args.serve_seconds / 2)
     two.update({"arrival_hz": rate, "capacity_hz": capacity,
-                "rate_rule": "80% of the capacity measured with 256 "
+                "rate_rule": "60% of the capacity measured with 256 "
                              "requests queued at once",
                 "chunk": loop.chunk, "batch_work": loop.batch_work,
                 "one_slot": {k: one[k] for k in ("requests", "p50_ms",
                                                  "p99_ms", "throughput",
+                                                 "inflight_frac",
                                                  "device_time_frac")}})
     return two
 

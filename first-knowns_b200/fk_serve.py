@@ -99,10 +99,15 @@ class ServeLoop:
         nxt = 0
         t0 = time.perf_counter()
         busy_s = 0.0
+        inflight_s = 0.0                        # wall time with a batch out
+        last = 0.0
         batches = 0
         work_done = 0
         while nxt < n or queue or inflight:
             now = time.perf_counter() - t0
+            if inflight:
+                inflight_s += now - last
+            last = now
             if time_limit is not None and now > time_limit and not inflight:
                 break
             while nxt < n and requests[nxt][0] <= now:
@@ -162,7 +167,7 @@ class ServeLoop:
         served = ~np.isnan(latency)
         stats = {"requests": int(served.sum()), "batches": batches,
                  "wall_s": wall, "device_busy_s": busy_s,
-                 "line_units": work_done}
+                 "inflight_s": inflight_s, "line_units": work_done}
         return results, latency, stats
 
     def _join(self, iv, parts):
