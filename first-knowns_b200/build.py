@@ -19,9 +19,10 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
     "-Xptxas", "-v",
 ]
+OBJ = HERE / "_obj"
 
 
 def sources():
@@ -38,20 +39,42 @@ def needs_build():
 
 
 def build(force=False, verbose=False):
-    """Compile libfk.so if any source is newer than it (or force)."""
+    """Compile libfk.so if any source is newer than it (or force): every
+    translation unit in csrc/ to an object, in parallel (the kernel
+    variants sit in units of their own), then one shared-library link."""
     if not force and not needs_build():
         return LIB
-    cmd = [NVCC] + FLAGS + ["-o", str(LIB) + ".tmp",
-                            str(CSRC / "fk_engine.cu"),
-                            str(CSRC / "fk_noalloc.cu")]
-    res = subprocess.run(cmd, capture_output=True, text=True)
-    log = res.stdout + res.stderr
-    (HERE / "build.log").write_text(log)
-    if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + log[-6000:])
+    OBJ.mkdir(exist_ok=True)
+    units = sorted(CSRC.glob("*.cu"))
+    jobs = []
+    for cu in units:
+        obj = OBJ / (cu.stem + ".o")
+        cmd = [NVCC] + FLAGS + ["-c", "-o", str(obj), str(cu)]
+        jobs.append((cu, obj, subprocess.Popen(
+            cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+            text=True)))
+    log, failed = [], []
+    for cu, obj, proc in jobs:
+        out = proc.communicate()[0]
+        log.append(f"== {cu.name}\n{out}")
+        if proc.returncode != 0:
+            failed.append(cu.name)
+    if not failed:
+        cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a",
+               "-shared", "-o", str(LIB) + ".tmp"] + \
+              [str(o) for _, o, _ in jobs]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        log.append("== link\n" + res.stdout + res.stderr)
+        if res.returncode != 0:
+            failed.append("link")
+    text = "".join(log)
+    (HERE / "build.log").write_text(text)
+    if failed:
+        raise RuntimeError("nvcc failed (" + ", ".join(failed) + "):\n" +
+                           text[-6000:])
     os.replace(str(LIB) + ".tmp", LIB)
     if verbose:
-        print(log)
+        print(text)
     return LIB
 
 

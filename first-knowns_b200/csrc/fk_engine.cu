@@ -17,6 +17,7 @@
 #include "fk_arith.cuh"
 #include "fk_classify.cuh"
 #include "fk_internal.h"
+#include "fk_launch.h"
 #include "fk_mark.cuh"
 #include "fk_sieve.cuh"
 #include "fk_types.h"
@@ -136,7 +137,12 @@ struct fk_engine {
                               // every sieve prime (f_q forbidden residues)
   bool use_mark = false;      // long lanes go to the marking sieve
   bool force_mark = false;    // every item goes to the marking sieve
-  std::vector<u32> mprefix;   // marking work entries before each marked prime
+  // per segment length (index seg_index(SEG)): marking work entries before
+  // each prime from index kNSMin, and the device tables (mq, mitems)
+  std::vector<u32> mprefix[kNumSeg];
+  std::vector<u64> mresidues[kNumSeg];  // residue walks before each prime
+  const uint64_t* d_mq[kNumSeg] = {};
+  const uint32_t* d_mitems[kNumSeg] = {};
   Cost cost;                  // cost model with every prime below 2^16 marked
   DevEngine dev{};
   std::vector<void*> allocs;
@@ -148,10 +154,10 @@ struct fk_engine {
 };
 
 // End of the marked prime range: primes below 2^16 (their lane shifts are
-// stored as u16), at most 8192 of them past the pattern primes.
+// stored as u16), at most kMarkPrimes of them from pattern prime kNSMin.
 static u32 NS_marked_end(const fk_engine* e) {
-  u32 i = kNS;
-  while (i < e->sieve.size() && e->sieve[i] < 65536u && i - kNS < (u32)kMarkPrimes) ++i;
+  u32 i = kNSMin;
+  while (i < e->sieve.size() && e->sieve[i] < 65536u && i - kNSMin < (u32)kMarkPrimes) ++i;
   return i;
 }
 
@@ -208,32 +214,43 @@ static fk_status upload(fk_engine* e, const std::vector<T>& h, const D** dptr,
   return FK_OK;
 }
 
+// Bytes of the engine's pattern tables (the first kNSMax pattern primes).
 static u32 pat_bytes_for(u32 P0) {
   switch (P0) {
-    case 6: return pat_bytes<6>();
-    case 7: return pat_bytes<7>();
-    case 9: return pat_bytes<9>();
-    default: return pat_bytes<11>();
+    case 6: return pat_bytes<6, kNSMax>();
+    case 7: return pat_bytes<7, kNSMax>();
+    case 9: return pat_bytes<9, kNSMax>();
+    default: return pat_bytes<11, kNSMax>();
   }
 }
 
-// Both kernels run the same pattern stage; the rounds then test each
-// pattern survivor against every remaining prime until one kills it; the
-// marking sieve pays about 1.5 instructions per byte mark plus, per
-// segment, one setup per work entry and an offset step per marked prime,
-// and per lane (task) the shift of every marked prime; candidates that
-// survive the marked primes are tested one by one against the rest.
-static Cost engine_cost(const fk_engine* e, u32 NPm) {
+// Both kernels run the same pattern stage (NS primes); the rounds then
+// test each pattern survivor against every remaining prime until one kills
+// it; the marking sieve pays about 1.5 instructions per byte mark plus,
+// per segment of SEG periods, one setup per work entry, an offset step per
+// marked prime and the map's zeroing and extraction, and per lane (task)
+// the shift of every marked prime; candidates that survive the marked
+// primes are tested one by one against the rest.
+static Cost engine_cost(const fk_engine* e, u32 NPm, u32 ns_sieve, u32 ns,
+                        u32 seg) {
   Cost c;
   const u32 NP = (u32)e->sieve.size();
-  double s1 = 1.0;
-  for (u32 i = 0; i < (u32)kNS && i < NP; ++i)
-    s1 *= 1.0 - (double)e->forb[i].size() / e->sieve[i];
-  double tests = 0, surv = 1.0, mark_bit = 0, tail = 0, surv_m = 1.0;
-  for (u32 i = kNS; i < NP; ++i) {
-    const double kill = (double)e->forb[i].size() / e->sieve[i];
+  // compaction rounds: pattern survival over ns_sieve primes, then tests
+  double s1r = 1.0;
+  for (u32 i = 0; i < ns_sieve && i < NP; ++i)
+    s1r *= 1.0 - (double)e->forb[i].size() / e->sieve[i];
+  double tests = 0, surv = 1.0;
+  for (u32 i = ns_sieve; i < NP; ++i) {
     tests += surv;
-    surv *= 1.0 - kill;
+    surv *= 1.0 - (double)e->forb[i].size() / e->sieve[i];
+  }
+  // marking: ns pattern primes, marks for [ns, NPm), tests past NPm
+  double s1 = 1.0;
+  for (u32 i = 0; i < ns && i < NP; ++i)
+    s1 *= 1.0 - (double)e->forb[i].size() / e->sieve[i];
+  double mark_bit = 0, tail = 0, surv_m = 1.0;
+  for (u32 i = ns; i < NP; ++i) {
+    const double kill = (double)e->forb[i].size() / e->sieve[i];
     if (i < NPm) {
       mark_bit += kill;
     } else {
@@ -241,29 +258,35 @@ static Cost engine_cost(const fk_engine* e, u32 NPm) {
     }
     surv_m *= 1.0 - kill;
   }
-  const double npm = NPm > (u32)kNS ? NPm - kNS : 0;
-  const double items = NPm > (u32)kNS && !e->mprefix.empty()
-                           ? e->mprefix[NPm - kNS] : 0;
-  c.round = 2.5 + 22.0 * s1 * tests;
+  const double npm = NPm > ns ? NPm - ns : 0;
+  const std::vector<u32>& mp = e->mprefix[seg_index(seg)];
+  const std::vector<u64>& mr = e->mresidues[seg_index(seg)];
+  const double items = NPm > ns && !mp.empty()
+                           ? (double)mp[NPm - kNSMin] - mp[ns - kNSMin] : 0;
+  const double walks = NPm > ns && !mr.empty()
+                           ? (double)mr[NPm - kNSMin] - mr[ns - kNSMin] : 0;
+  c.round = 2.5 + 22.0 * s1r * tests;
   c.bit = 2.5 + 2.0 + 1.5 * mark_bit + 22.0 * s1 * tail;
-  c.seg = 12.0 * items + 6.0 * npm + 2048.0;
+  c.seg = 16.0 * items + 8.0 * walks + 6.0 * npm + 2048.0 * seg / 32768.0;
   c.lane = 25.0 * npm;
-  c.mark = NPm > (u32)kNS;
+  c.mark = NPm > ns;
   return c;
 }
 
-// Prime-index cuts of the compaction rounds: a round ends once the
-// modelled survival of a candidate within it falls below `cut` (or after
-// 4096 primes), so the ballot compaction between rounds runs when about
-// 1 - cut of the lanes have gone idle; at most kMaxRounds rounds.
+// Prime-index cuts of the compaction rounds over the primes past the ns
+// pattern primes: a round ends once the modelled survival of a candidate
+// within it falls below `cut` (or after 4096 primes), so the ballot
+// compaction between rounds runs when about 1 - cut of the lanes have gone
+// idle; at most kMaxRounds rounds.
 static constexpr double kDefaultRoundCut = 0.5;
-static std::vector<u32> compute_rounds(const fk_engine* e, double cut) {
+static std::vector<u32> compute_rounds(const fk_engine* e, double cut,
+                                       u32 ns) {
   const u32 NP = (u32)e->sieve.size();
   std::vector<u32> rounds;
-  rounds.push_back(kNS);
+  rounds.push_back(ns);
   double s = 1.0;
-  u32 start = kNS;
-  for (u32 i = kNS; i < NP; ++i) {
+  u32 start = ns;
+  for (u32 i = ns; i < NP; ++i) {
     s *= 1.0 - (double)e->forb[i].size() / e->sieve[i];
     if ((s < cut || i + 1 - start >= 4096) && i + 1 < NP) {
       rounds.push_back(i + 1);
@@ -276,8 +299,21 @@ static std::vector<u32> compute_rounds(const fk_engine* e, double cut) {
     rounds.resize(kMaxRounds);
     rounds.push_back(NP);
   }
-  if (NP <= (u32)kNS) rounds.assign({(u32)kNS, (u32)kNS});
+  if (NP <= ns) rounds.assign({ns, ns});
   return rounds;
+}
+
+// Point a descriptor at the marking tables of segment length seg, from
+// the first prime past ns pattern primes to npm (exclusive).
+static void set_mark_tables(const fk_engine* e, DevEngine& d, u32 ns,
+                            u32 seg, u32 npm) {
+  const int si = seg_index(seg);
+  const std::vector<u32>& mp = e->mprefix[si];
+  d.NS = ns;
+  d.NPm = npm;
+  d.mq = e->d_mq[si];
+  d.mitems = e->d_mitems[si] + 4 * (npm > ns ? mp[ns - kNSMin] : 0);
+  d.nmitems = npm > ns ? mp[npm - kNSMin] - mp[ns - kNSMin] : 0;
 }
 
 static fk_status build_engine(fk_engine* e) {
@@ -297,7 +333,7 @@ static fk_status build_engine(fk_engine* e) {
     return set_err(FK_ERR_DOMAIN, "p0 must be 6, 7, 9 or 11");
   e->P0 = P0;
   const u32 first_pat = fk_nth_prime((int)P0);
-  const u32 last_pat = fk_nth_prime((int)P0 + kNS - 1);
+  const u32 last_pat = fk_nth_prime((int)P0 + kNSMax - 1);
   if (e->q2 <= last_pat + 1)
     return set_err(FK_ERR_DOMAIN, "q2 " + std::to_string(e->q2) +
                                       " is too small for the pattern sieve "
@@ -361,14 +397,15 @@ static fk_status build_engine(fk_engine* e) {
     e->forb.push_back(is_sieve_prime(e, q) ? forbidden(e, q) : std::vector<u32>());
   }
   const u32 NP = (u32)e->sieve.size();
-  // ---- pattern tables (the first kNS sieve primes) -----------------------
+  // ---- pattern tables (the first kNSMax sieve primes; a kernel variant
+  // stages the first NS of them) ---------------------------------------------
   // entry k of prime q's table is the mask of the 64 periods from phase
   // rho = 64k mod q, so a lane's consecutive words are consecutive entries
   // and the 32 lanes of a warp sweeping one lane read 32 consecutive
   // entries (no bank conflict)
   std::vector<u64> pat;
-  std::vector<u32> minv(kNS), i64(kNS);
-  for (int i = 0; i < kNS; ++i) {
+  std::vector<u32> minv(kNSMax), i64(kNSMax);
+  for (int i = 0; i < kNSMax; ++i) {
     const u32 q = e->sieve[i];
     if (q != fk_nth_prime((int)P0 + i))
       return set_err(FK_ERR_DEVICE, "pattern prime layout mismatch");
@@ -418,7 +455,7 @@ static fk_status build_engine(fk_engine* e) {
       const u64 dq = (u64)(e->d % q);
       r.aux = dq ? (u32)invmod(dq, q) : 0;
     }
-    if (use_list && i >= (u32)kNS) {
+    if (use_list && i >= (u32)kNSMin) {
       std::vector<u32> lf = f;
       if (e->kind == KIND_DICKSON) {
         // the roots come in pairs x, q - x: keep min(x, q - x) and a 64-bit
@@ -436,10 +473,10 @@ static fk_status build_engine(fk_engine* e) {
     }
     recs[i] = r;
   }
-  for (u32 i = kNS; i < NP; ++i)
+  for (u32 i = kNSMax; i < NP; ++i)
     e->survival *= 1.0 - (double)e->forb[i].size() / e->sieve[i];
   // ---- compaction rounds: a round ends when survival within it halves ----
-  const std::vector<u32> rounds = compute_rounds(e, kDefaultRoundCut);
+  const std::vector<u32> rounds = compute_rounds(e, kDefaultRoundCut, kNS);
   // ---- marking tables: u-residue lists for every prime, (M mod q)^-1 ------
   std::vector<u32> minv_all(NP), gaux(NP), glist;
   u32 NPm = NS_marked_end(e);
@@ -456,30 +493,56 @@ static fk_status build_engine(fk_engine* e) {
     glist.insert(glist.end(), g.begin(), g.end());
   }
   if (glist.size() >= (1u << 24)) return set_err(FK_ERR_DOMAIN, "glist too large");
-  // ---- marking work list: every (prime, forbidden residue) progression
-  // cut into sub-ranges of at least kMarkHits hits and at most 8 per
-  // segment, ordered by prime so a warp's entries share q and trip counts
-  std::vector<u64> mq;
-  std::vector<u64> mitems;
-  for (u32 i = kNS; i < NPm; ++i) {
-    const u32 q = e->sieve[i];
-    const u32 pi = i - kNS;
-    u32 S = 0, nsub = 1;
-    if (q < (u32)(kSeg / kMarkHits)) {
-      const u32 K = std::max<u32>(kMarkHits, ((u32)kSeg / 8 + q - 1) / q);
-      S = K * q;
-      nsub = ((u32)kSeg + S - 1) / S;
-    }
-    mq.push_back((u64)q | ((u64)((u32)kSeg % q) << 16) | ((u64)S << 32));
-    e->mprefix.push_back((u32)mitems.size());
+  // ---- marking residue lists: each marked prime's forbidden period
+  // residues as u16, padded to a multiple of four (one 8-byte load each)
+  std::vector<uint16_t> mres;
+  std::vector<u32> mres_at(NP, 0);
+  for (u32 i = kNSMin; i < NPm; ++i) {
+    mres_at[i] = (u32)mres.size();
     const u32 go = gaux[i] & 0x00FFFFFFu, gc = gaux[i] >> 24;
-    for (u32 k = 0; k < nsub; ++k)
-      for (u32 c = 0; c < gc; ++c)
-        mitems.push_back((u64)(glist[go + c] | (pi << 16) | (k << 29)) |
-                         ((u64)q << 32) | ((u64)S << 48));
+    for (u32 c = 0; c < gc; ++c) mres.push_back((uint16_t)glist[go + c]);
+    while (mres.size() % 4) mres.push_back(0xFFFFu);
   }
-  e->mprefix.push_back((u32)mitems.size());
-  e->cost = engine_cost(e, NPm);
+  if (mres.size() >= (1u << 26)) return set_err(FK_ERR_DOMAIN, "mres too large");
+  // ---- marking work lists, one per segment length SEG: one entry per
+  // (prime, sub-range) from prime index kNSMin, each walking all of its
+  // prime's residues; small primes are cut into sub-ranges of at least
+  // kMarkHits hits per residue and at most 8 per segment, so the heavy
+  // primes spread over the threads.  Ordered by prime: a warp's entries
+  // share q, residue count and trip counts.
+  std::vector<u64> mq[kNumSeg];
+  std::vector<u32> mitems[kNumSeg];   // four words per entry
+  for (int si = 0; si < kNumSeg; ++si) {
+    const u32 seg = (u32)kSegOf(si);
+    e->mprefix[si].clear();
+    e->mresidues[si].clear();
+    u64 nres = 0;
+    for (u32 i = kNSMin; i < NPm; ++i) {
+      const u32 q = e->sieve[i];
+      const u32 pi = i - kNSMin;
+      u32 S = 0, nsub = 1;
+      if (q < seg / kMarkHits) {
+        const u32 K = std::max<u32>(kMarkHits, (seg / 8 + q - 1) / q);
+        S = K * q;
+        nsub = (seg + S - 1) / S;
+      }
+      mq[si].push_back((u64)q | ((u64)(seg % q) << 16));
+      e->mprefix[si].push_back((u32)(mitems[si].size() / 4));
+      e->mresidues[si].push_back(nres);
+      const u32 gc = gaux[i] >> 24;
+      if (gc == 0) continue;
+      for (u32 k = 0; k < nsub; ++k) {
+        mitems[si].push_back(pi | (k << 13));
+        mitems[si].push_back(q | (S << 16));
+        mitems[si].push_back((mres_at[i] / 4) | (gc << 24));
+        mitems[si].push_back(0);
+        nres += gc;
+      }
+    }
+    e->mprefix[si].push_back((u32)(mitems[si].size() / 4));
+    e->mresidues[si].push_back(nres);
+  }
+  e->cost = engine_cost(e, NPm, kNS, kNS, kSeg);
   e->use_mark = e->cost.mark;
   if (p.sieve == 1) e->use_mark = false;
   e->force_mark = p.sieve == 2 && e->use_mark;
@@ -513,12 +576,17 @@ static fk_status build_engine(fk_engine* e) {
   if ((st = upload(e, sbits, &d.sbits))) return st;
   d.NPm = NPm;
   d.use_mark = e->use_mark ? 1 : 0;
-  d.nmitems = (u32)mitems.size();
   if ((st = upload(e, minv_all, &d.minv_all))) return st;
   if ((st = upload(e, gaux, &d.gaux))) return st;
   if ((st = upload(e, glist, &d.glist))) return st;
-  if ((st = upload(e, mq, &d.mq))) return st;
-  if ((st = upload(e, mitems, &d.mitems))) return st;
+  if ((st = upload(e, mres, &d.mres))) return st;
+  for (int si = 0; si < kNumSeg; ++si) {
+    if ((st = upload(e, mq[si], &e->d_mq[si]))) return st;
+    if ((st = upload(e, mitems[si], &e->d_mitems[si]))) return st;
+  }
+  // the engine's own descriptor: the default variant (kNS pattern primes,
+  // kSeg-period segments)
+  set_mark_tables(e, d, kNS, kSeg, NPm);
   return FK_OK;
 }
 
@@ -634,10 +702,12 @@ struct fk_batch {
 static const fk_tuning kDefaultTuning = {3, 3, 2048, (u32)kWarpMode,
                                          (u32)kSegPerTask, 8, 65536, 1.0f,
                                          256, 1.0f,
-                                         (float)kDefaultRoundCut, 32};
+                                         (float)kDefaultRoundCut, 32,
+                                         (u32)kSeg, (u32)kNS, (u32)kNS};
 
-// Upload this batch's copy of every engine descriptor with the marked
-// prime range cut at tune.mark_limit, and the matching cost models.
+// Upload this batch's copy of every engine descriptor: the kernel
+// variant's pattern-prime count and segment tables, the marked prime range
+// cut at tune.mark_limit, the round cuts, and the matching cost models.
 static fk_status apply_tuning(fk_batch* b) {
   const u32 ne = (u32)b->engines.size();
   std::vector<DevEngine> de(ne);
@@ -647,7 +717,8 @@ static fk_status apply_tuning(fk_batch* b) {
   std::vector<std::vector<u32>> rounds(ne);
   std::vector<u32> flat;
   for (u32 i = 0; i < ne; ++i) {
-    rounds[i] = compute_rounds(b->engines[i], b->tune.round_cut);
+    rounds[i] = compute_rounds(b->engines[i], b->tune.round_cut,
+                               b->tune.pattern_primes);
     flat.insert(flat.end(), rounds[i].begin(), rounds[i].end());
   }
   fk_status rs = b->d_rounds.ensure(flat.size());
@@ -658,12 +729,13 @@ static fk_status apply_tuning(fk_batch* b) {
   for (u32 i = 0; i < ne; ++i) {
     const fk_engine* e = b->engines[i];
     DevEngine d = e->dev;
+    const u32 ns = b->tune.mark_pattern_primes, seg = b->tune.mark_segment;
     u32 npm = d.NPm;
-    while (npm > (u32)kNS && e->sieve[npm - 1] >= b->tune.mark_limit) --npm;
-    d.NPm = npm;
-    d.nmitems = npm > (u32)kNS ? e->mprefix[npm - kNS] : 0;
-    b->cost[i] = npm == e->dev.NPm ? e->cost : engine_cost(e, npm);
-    b->mark_ok[i] = e->use_mark && npm > (u32)kNS;
+    while (npm > ns && e->sieve[npm - 1] >= b->tune.mark_limit) --npm;
+    if (npm < ns) npm = ns;
+    set_mark_tables(e, d, ns, seg, npm);
+    b->cost[i] = engine_cost(e, npm, b->tune.pattern_primes, ns, seg);
+    b->mark_ok[i] = e->use_mark && npm > ns;
     d.use_mark = b->mark_ok[i];
     d.rounds = b->d_rounds.p + roff;
     d.nrounds = (u32)rounds[i].size() - 1;
@@ -699,22 +771,8 @@ static fk_status batch_init(fk_batch* b, fk_engine* const* engines,
   FK_CUDA(b->h_ctr.ensure(1) == FK_OK ? cudaSuccess : cudaErrorMemoryAllocation);
   static bool attrs_done = false;
   if (!attrs_done) {
-    FK_CUDA(cudaFuncSetAttribute(k_sieve<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(pat_bytes<7>() + sizeof(SieveSmem))));
-    FK_CUDA(cudaFuncSetAttribute(k_sieve<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(pat_bytes<6>() + sizeof(SieveSmem))));
-    FK_CUDA(cudaFuncSetAttribute(k_sieve<9>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(pat_bytes<9>() + sizeof(SieveSmem))));
-    FK_CUDA(cudaFuncSetAttribute(k_sieve<11>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(pat_bytes<11>() + sizeof(SieveSmem))));
-    FK_CUDA(cudaFuncSetAttribute(k_mark<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(pat_bytes<7>() + sizeof(MarkSmem))));
-    FK_CUDA(cudaFuncSetAttribute(k_mark<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(pat_bytes<6>() + sizeof(MarkSmem))));
-    FK_CUDA(cudaFuncSetAttribute(k_mark<9>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(pat_bytes<9>() + sizeof(MarkSmem))));
-    FK_CUDA(cudaFuncSetAttribute(k_mark<11>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(pat_bytes<11>() + sizeof(MarkSmem))));
+    FK_CUDA(sieve_set_smem_limits());
+    FK_CUDA(mark_set_smem_limits());
     attrs_done = true;
   }
   return FK_OK;
@@ -778,7 +836,8 @@ static fk_status expand(fk_batch* b, const fk_item* items, u64 nitems) {
   b->sieve_idx.clear();
   for (auto& f : b->fam) { f.idx.clear(); f.prefix.assign(1, 0); }
   const u64 target_chains = (u64)b->nsm * b->tune.chains_per_sm;
-  const u64 seg_task = (u64)kSeg * b->tune.seg_per_task;
+  const u64 seg_len = b->tune.mark_segment;
+  const u64 seg_task = seg_len * b->tune.seg_per_task;
   for (u64 ui = 0; ui < nitems; ++ui) {
     const fk_item& it = items[ui];
     if (it.engine >= b->engines.size())
@@ -833,7 +892,7 @@ static fk_status expand(fk_batch* b, const fk_item* items, u64 nitems) {
         const double Ud = (double)U;
         const double rounds = Ud * c.round;
         const double tasks = std::ceil(Ud / (double)seg_task);
-        const double segs = std::ceil(Ud / kSeg);
+        const double segs = std::ceil(Ud / (double)seg_len);
         const double marking = tasks * c.lane + segs * c.seg + Ud * c.bit;
         mark = e->force_mark || marking < (double)b->tune.mark_bias * rounds;
       }
@@ -985,23 +1044,11 @@ static fk_status enqueue(fk_batch* b, bool capturing = false) {
                                        : b->tune.sieve_ctas_per_sm));
     ++nl;
     const u32 P0 = F.P0;
-    if (F.mark) {
-      const size_t sm = pat_bytes_for(P0) + sizeof(MarkSmem);
-      switch (P0) {
-        case 7: k_mark<7><<<(u32)grid, kBlock, sm, s>>>(a); break;
-        case 6: k_mark<6><<<(u32)grid, kBlock, sm, s>>>(a); break;
-        case 9: k_mark<9><<<(u32)grid, kBlock, sm, s>>>(a); break;
-        default: k_mark<11><<<(u32)grid, kBlock, sm, s>>>(a); break;
-      }
-    } else {
-      const size_t sm = pat_bytes_for(P0) + sizeof(SieveSmem);
-      switch (P0) {
-        case 7: k_sieve<7><<<(u32)grid, kBlock, sm, s>>>(a); break;
-        case 6: k_sieve<6><<<(u32)grid, kBlock, sm, s>>>(a); break;
-        case 9: k_sieve<9><<<(u32)grid, kBlock, sm, s>>>(a); break;
-        default: k_sieve<11><<<(u32)grid, kBlock, sm, s>>>(a); break;
-      }
-    }
+    if (F.mark)
+      FK_CUDA(launch_mark(P0, b->tune.mark_pattern_primes,
+                          b->tune.mark_segment, (u32)grid, s, a));
+    else
+      FK_CUDA(launch_sieve(P0, b->tune.pattern_primes, (u32)grid, s, a));
     FK_CUDA(record(b->fev[2 * f + 1], s, capturing));
   }
   FK_CUDA(cudaGetLastError());
@@ -1101,6 +1148,8 @@ static fk_status launch(fk_batch* b, int use_graph) {
   key.push_back(((u64)b->tune.sieve_ctas_per_sm << 32) | b->tune.mark_ctas_per_sm);
   key.push_back(((u64)b->tune.warp_queue << 32) | b->tune.seg_per_task);
   key.push_back(b->tune.classify_ctas_per_sm);
+  key.push_back(((u64)b->tune.pattern_primes << 48) |
+                ((u64)b->tune.mark_pattern_primes << 32) | b->tune.mark_segment);
   if (b->gexec == nullptr || key != b->graph_key) {
     if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
     if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
@@ -1233,7 +1282,7 @@ fk_status fk_engine_info(const fk_engine* e, fk_info* out) {
   out->nrounds = e->dev.nrounds;
   out->device_bytes = e->device_bytes;
   out->use_mark = e->use_mark ? 1 : 0;
-  out->marked_primes = e->dev.NPm > (u32)kNS ? e->dev.NPm - kNS : 0;
+  out->marked_primes = e->dev.NPm > e->dev.NS ? e->dev.NPm - e->dev.NS : 0;
   out->survival = e->survival;
   return FK_OK;
 }
@@ -1406,6 +1455,15 @@ fk_status fk_batch_set_tuning(fk_batch* b, const fk_tuning* t) {
   if (t->capacity_scale > 0.0f) n.capacity_scale = t->capacity_scale;
   if (t->round_cut > 0.0f) n.round_cut = t->round_cut;
   if (t->group_lane_words) n.group_lane_words = t->group_lane_words;
+  if (t->mark_segment) n.mark_segment = t->mark_segment;
+  if (t->pattern_primes) n.pattern_primes = t->pattern_primes;
+  if (t->mark_pattern_primes) n.mark_pattern_primes = t->mark_pattern_primes;
+  if (!valid_mark_segment(n.mark_segment) ||
+      !valid_pattern_primes(n.pattern_primes) ||
+      !valid_pattern_primes(n.mark_pattern_primes))
+    return set_err(FK_ERR_DOMAIN,
+                   "mark_segment must be 16384, 32768 or 65536 and "
+                   "pattern_primes, mark_pattern_primes 24, 32 or 40");
   if (!(n.capacity_scale >= 1e-4f && n.capacity_scale <= 1e3f) ||
       !(n.round_cut >= 0.05f && n.round_cut <= 0.95f))
     return set_err(FK_ERR_DOMAIN, "tuning value out of range");

@@ -4,23 +4,25 @@
 // candidates alive deep into the prime list, and testing each of them
 // against every remaining prime costs tens of tests per candidate.  Long
 // lanes are therefore sieved the Eratosthenes way instead: one CTA owns one
-// lane over kSeg * seg_per_task consecutive periods, and per segment of
-// kSeg periods it
-//   (a) ORs the compile-time pattern primes into two words per thread
-//       (the stage-1a pattern sieve of fk_sieve.cuh),
-//   (b) marks every other prime below 2^16 into a kSeg-byte shared map.
-//       Each (prime, forbidden residue) progression of step q is one or
-//       more work entries of at least kMarkHits hits, built once per
-//       engine and ordered by prime; the threads take the entries round
-//       robin, so the heavy small primes spread over every warp and a
-//       warp's entries share q and trip count.  Marks are plain byte
-//       stores (a mark is idempotent: no read-modify-write, no atomic),
-//       four per loop trip, and
+// lane over SEG * seg_per_task consecutive periods, and per segment of SEG
+// periods (16384, 32768 or 65536: a template variant chosen per batch) it
+//   (a) ORs the NS compile-time pattern primes into SEG / 16384 words per
+//       thread (the stage-1a pattern sieve of fk_sieve.cuh),
+//   (b) marks every other prime below 2^16 into a SEG-byte shared map.
+//       A work entry is one prime (or, for the small primes, one
+//       sub-range of at least kMarkHits hits per residue): it sets up the
+//       prime's offset and bounds once and then writes the progression of
+//       step q of each of the prime's forbidden residues.  Entries are
+//       built once per engine and ordered by prime; the threads take them
+//       round robin, so the heavy small primes spread over every warp and
+//       a warp's entries share q, residue count and trip counts.  Marks
+//       are plain byte stores (a mark is idempotent: no read-modify-write,
+//       no atomic), four per loop trip, and
 //   (c) extracts the periods that neither marked, tests any primes beyond
 //       the marked range one by one, and appends the survivors to the
 //       candidate list.
 // Each prime's first hit offset lives in shared memory and steps by the
-// tabulated kSeg mod q from one segment to the next.
+// tabulated SEG mod q from one segment to the next.
 // This is the reference AP engine's bitmap marking (primorial-ap/ap_gpu.py:
 // 204-369: tabulated small primes, shared-memory marks for mid primes,
 // global atomics for the rest) re-laid out per lane, so no mark needs an
@@ -30,13 +32,15 @@
 
 namespace fk {
 
+template <int SEG>
 struct MarkSmem {
-  unsigned char bytes[kSeg];
-  unsigned short off16[kMarkPrimes];  // first hit offset of each marked prime
-  u32 ph[kNS];                        // table index at the segment start
-  u32 lsh[kNS];                       // the lane's index shift per prime
+  unsigned char bytes[SEG];
+  unsigned short off16[kMarkPrimes];  // first hit offset of each prime from
+                                      // index kNSMin (marked ones are used)
+  u32 ph[kNSMax];                     // table index at the segment start
+  u32 lsh[kNSMax];                    // the lane's index shift per prime
   u32 warp[kBlock / 32];
-  u32 minv[kNS];
+  u32 minv[kNSMax];
   u32 sbits[512];
   u64 task;
   u32 item;
@@ -46,30 +50,32 @@ struct MarkSmem {
   unsigned long long mbar;
 };
 
-// The two pattern words of thread t in a segment (words 2t and 2t + 1),
-// from each prime's table index at the segment start in shared memory
-// (ph[I]; consecutive words are consecutive entries): no per-prime index
-// occupies a register while the segment is marked.
-template <int P0, int I, int NS>
+// The WPT pattern words of thread t in a segment (words WPT*t ...
+// WPT*t + WPT - 1), from each prime's table index at the segment start in
+// shared memory (ph[I]; consecutive words are consecutive entries): no
+// per-prime index occupies a register while the segment is marked.
+template <int P0, int I, int NS, int WPT>
 struct PatSeg {
   static __device__ __forceinline__ void words(const u64* __restrict__ spat,
-                                               const u32* ph, u32 t2,
-                                               u64& acc0, u64& acc1) {
+                                               const u32* ph, u32 tw,
+                                               u64* acc) {
     constexpr u32 q = fk_nth_prime(P0 + I);
     constexpr u32 off = fk_pat_prefix(P0, I);
-    u32 r = ph[I] + t2 % q;
+    u32 r = ph[I] + tw % q;
     r = min(r, r - q);
-    acc0 |= spat[off + r];
-    u32 r2 = r + 1;
-    r2 = min(r2, r2 - q);
-    acc1 |= spat[off + r2];
-    PatSeg<P0, I + 1, NS>::words(spat, ph, t2, acc0, acc1);
+#pragma unroll
+    for (int k = 0; k < WPT; ++k) {
+      acc[k] |= spat[off + r];
+      r += 1;
+      r = min(r, r - q);
+    }
+    PatSeg<P0, I + 1, NS, WPT>::words(spat, ph, tw, acc);
   }
 };
-template <int P0, int NS>
-struct PatSeg<P0, NS, NS> {
+template <int P0, int NS, int WPT>
+struct PatSeg<P0, NS, NS, WPT> {
   static __device__ __forceinline__ void words(const u64*, const u32*, u32,
-                                               u64&, u64&) {}
+                                               u64*) {}
 };
 
 template <int KIND>
@@ -88,11 +94,16 @@ __device__ __forceinline__ bool tail_alive(u64 v, const DevEngine& e,
   return true;
 }
 
-template <int P0>
+// NS pattern primes, SEG periods per segment; the engine descriptor's NS
+// and marking tables (mq, mitems) must be the ones of this variant.
+template <int P0, int NS, int SEG>
 __global__ void __launch_bounds__(kBlock, 3) k_mark(SieveArgs a) {
+  constexpr int WPT = SEG / (64 * kBlock);  // pattern words per thread
+  static_assert(WPT * 64 * kBlock == SEG, "segment must be 1-4 words per thread");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   u64* spat = reinterpret_cast<u64*>(smem_raw);
-  MarkSmem& S = *reinterpret_cast<MarkSmem*>(smem_raw + pat_bytes<P0>());
+  MarkSmem<SEG>& S =
+      *reinterpret_cast<MarkSmem<SEG>*>(smem_raw + pat_bytes<P0, NS>());
   const int tid = threadIdx.x;
   if (tid == 0) {
     S.eng = 0xFFFFFFFFu;
@@ -127,9 +138,9 @@ __global__ void __launch_bounds__(kBlock, 3) k_mark(SieveArgs a) {
     const u32 eidx = it.engine;
     const DevEngine& eg = a.engines[eidx];
     if (S.eng != eidx) {
-      if (!stage_patterns<P0>(spat, eg, &S.mbar, &S.status, phase, a.ctr))
+      if (!stage_patterns<P0, NS>(spat, eg, &S.mbar, &S.status, phase, a.ctr))
         return;
-      for (u32 i = tid; i < kNS; i += kBlock) S.minv[i] = eg.pat_minv[i];
+      for (u32 i = tid; i < (u32)NS; i += kBlock) S.minv[i] = eg.pat_minv[i];
       for (u32 i = tid; i < eg.sbits_words && i < 512; i += kBlock)
         S.sbits[i] = eg.sbits[i];
       __syncthreads();
@@ -141,12 +152,13 @@ __global__ void __launch_bounds__(kBlock, 3) k_mark(SieveArgs a) {
     const u32 lane = (u32)(tl % e.L);
     const u64 chunk = tl / e.L;
     const u64 R = e.lanes[lane];
-    const u64 u_start = chunk * (u64)kSeg * a.seg_per_task;
-    const u64 u_end = min((u64)it.U, u_start + (u64)kSeg * a.seg_per_task);
-    const u32 npm = e.NPm - e.NS;   // marked primes (the batch's bound)
+    const u64 u_start = chunk * (u64)SEG * a.seg_per_task;
+    const u64 u_end = min((u64)it.U, u_start + (u64)SEG * a.seg_per_task);
+    // marked primes: indices [NS, NPm), off16 / mq slots [pbeg, pend)
+    const u32 pbeg = (u32)(NS - kNSMin), pend = e.NPm - kNSMin;
     // the lane's index shift and first-segment table index for every
     // pattern prime: ((u + s_l) * 64^-1) mod q, s_l carrying 64^-1 already
-    if (tid < kNS) {
+    if (tid < NS) {
       const PrimeRec pr = e.recs[tid];
       u32 x = xq[tid] + fk_bmod(R, pr.q, pr.magic);
       x = min(x, x - pr.q);
@@ -157,8 +169,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_mark(SieveArgs a) {
       S.ph[tid] = min(p, p - pr.q);
     }
     // the first hit offset of every marked prime in the first segment
-    for (u32 pi = tid; pi < npm; pi += kBlock) {
-      const u32 i = e.NS + pi;
+    for (u32 pi = pbeg + tid; pi < pend; pi += kBlock) {
+      const u32 i = kNSMin + pi;
       const PrimeRec pr = e.recs[i];
       u32 x = xq[i] + fk_bmod(R, pr.q, pr.magic);
       x = min(x, x - pr.q);
@@ -167,47 +179,64 @@ __global__ void __launch_bounds__(kBlock, 3) k_mark(SieveArgs a) {
       S.off16[pi] = (unsigned short)min(o, o - pr.q);
     }
     __syncthreads();
-    for (u64 useg = u_start; useg < u_end; useg += kSeg) {
-      const u32 seg_len = (u32)min((u64)kSeg, u_end - useg);
-      // (a) the pattern words 2*tid and 2*tid + 1
-      u64 acc0 = 0, acc1 = 0;
-      PatSeg<P0, 0, kNS>::words(spat, S.ph, 2u * (u32)tid, acc0, acc1);
-      nword += 2;
+    for (u64 useg = u_start; useg < u_end; useg += SEG) {
+      const u32 seg_len = (u32)min((u64)SEG, u_end - useg);
+      // (a) the pattern words WPT*tid ... WPT*tid + WPT - 1
+      u64 acc[WPT];
+#pragma unroll
+      for (int k = 0; k < WPT; ++k) acc[k] = 0;
+      PatSeg<P0, 0, NS, WPT>::words(spat, S.ph, (u32)(WPT * tid), acc);
+      nword += WPT;
       // zero the byte map
       {
         uint4* b4 = reinterpret_cast<uint4*>(S.bytes);
         const uint4 z = make_uint4(0, 0, 0, 0);
 #pragma unroll
-        for (int k = 0; k < kSeg / 16 / kBlock; ++k) b4[tid + k * kBlock] = z;
+        for (int k = 0; k < SEG / 16 / kBlock; ++k) b4[tid + k * kBlock] = z;
       }
       __syncthreads();
       // (b) mark: the work entries round robin over the threads, the next
-      // entry's load in flight while this one's progression is written
-      // (an entry carries its prime and sub-range length: one load each)
+      // entry's load in flight while this one is walked.  An entry is one
+      // prime's sub-range: its offset and bounds are set up once, then
+      // each forbidden residue's progression is written, four residues
+      // per 8-byte load of the residue list
       {
         const u32 nm = e.nmitems;
-        const u64* __restrict__ mit = reinterpret_cast<const u64*>(e.mitems);
+        const uint4* __restrict__ mit = reinterpret_cast<const uint4*>(e.mitems);
+        const uint2* __restrict__ mres = reinterpret_cast<const uint2*>(e.mres);
         unsigned char* __restrict__ B = S.bytes;
         u32 cnt = 0;
         u32 i = tid;
-        u64 w = i < nm ? __ldg(mit + i) : 0ull;
+        uint4 w = i < nm ? __ldg(mit + i) : make_uint4(0, 0, 0, 0);
         while (i < nm) {
           const u32 inext = i + kBlock;
-          const u64 wn = inext < nm ? __ldg(mit + inext) : 0ull;
-          const u32 wl = (u32)w, wh = (u32)(w >> 32);
-          const u32 g = wl & 0xFFFFu, pi = (wl >> 16) & 0x1FFFu, k = wl >> 29;
-          const u32 q = wh & 0xFFFFu, sl = wh >> 16;
+          const uint4 wn = inext < nm ? __ldg(mit + inext) : make_uint4(0, 0, 0, 0);
+          const u32 pi = w.x & 0x1FFFu, k = w.x >> 13;
+          const u32 q = w.y & 0xFFFFu, sl = w.y >> 16;
+          const u32 gslot = w.z & 0x00FFFFFFu, gc = w.z >> 24;
           const u32 off = S.off16[pi];
-          u32 h = (g >= off ? g - off : g + q - off) + k * sl;
-          const u32 end = sl ? min(seg_len, (k + 1) * sl) : seg_len;
+          const u32 base = k * sl;
+          const u32 end = sl ? min(seg_len, base + sl) : seg_len;
           const u32 q2 = 2 * q, q3 = 3 * q, q4 = 4 * q;
-          for (; h + q3 < end; h += q4, cnt += 4) {
-            B[h] = 1;
-            B[h + q] = 1;
-            B[h + q2] = 1;
-            B[h + q3] = 1;
+          for (u32 c = 0; c < gc; c += 4) {
+            const uint2 gg = __ldg(mres + gslot + (c >> 2));
+            const u32 gv[4] = {gg.x & 0xFFFFu, gg.x >> 16, gg.y & 0xFFFFu,
+                               gg.y >> 16};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              if (gv[j] == 0xFFFFu) break;   // the list's padding
+              const u32 d = gv[j] - off;
+              u32 h = min(d, d + q) + base;  // (g - off) mod q, then the
+                                             // sub-range's start
+              for (; h + q3 < end; h += q4, cnt += 4) {
+                B[h] = 1;
+                B[h + q] = 1;
+                B[h + q2] = 1;
+                B[h + q3] = 1;
+              }
+              for (; h < end; h += q, ++cnt) B[h] = 1;
+            }
           }
-          for (; h < end; h += q, ++cnt) B[h] = 1;
           i = inext;
           w = wn;
         }
@@ -216,23 +245,23 @@ __global__ void __launch_bounds__(kBlock, 3) k_mark(SieveArgs a) {
       __syncthreads();
       // advance the offsets and phases to the next segment (nothing below
       // reads them before the next segment's barrier)
-      if (useg + kSeg < u_end) {
-        for (u32 pi = tid; pi < npm; pi += kBlock) {
+      if (useg + SEG < u_end) {
+        for (u32 pi = pbeg + tid; pi < pend; pi += kBlock) {
           const u64 m = __ldg(reinterpret_cast<const u64*>(e.mq) + pi);
           const u32 q = (u32)m & 0xFFFFu;
           const u32 o = S.off16[pi] + (((u32)m >> 16) & 0xFFFFu);
           S.off16[pi] = (unsigned short)min(o, o - q);
         }
-        if (tid < kNS) {
+        if (tid < NS) {
           const PrimeRec pr = e.recs[tid];
-          const u32 p = S.ph[tid] + (u32)(kSeg / 64) % pr.q;
+          const u32 p = S.ph[tid] + (u32)(SEG / 64) % pr.q;
           S.ph[tid] = min(p, p - pr.q);
         }
       }
       // (c) extract
 #pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const u32 w = 2 * tid + k;
+      for (int k = 0; k < WPT; ++k) {
+        const u32 w = WPT * tid + k;
         const u64 uw = useg + 64ull * w;
         if (uw >= u_end) continue;
         const uint2* bw = reinterpret_cast<const uint2*>(S.bytes + 64 * w);
@@ -248,7 +277,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_mark(SieveArgs a) {
         if (uw == 0 && R < it.lo_off) valid &= ~1ull;
         if (it.U - uw <= 64 && R >= it.hi_last)
           valid &= ~(1ull << (it.U - uw - 1));
-        u64 surv = ~(k ? acc1 : acc0) & ~m & valid;
+        u64 surv = ~acc[k] & ~m & valid;
         while (surv) {
           const int b = __ffsll((long long)surv) - 1;
           surv &= surv - 1;

@@ -8,7 +8,7 @@
 // synchronisation an allocation can cause.  fk_sieve (fk_engine.cu) grows
 // its buffers on demand; this entry point instead keeps every piece of
 // per-call scratch -- the item descriptor, the base-residue table, the
-// candidate list, the counters and the sort buffer -- in one fixed array
+// candidate list, the counters and the ordering buffers -- in one fixed array
 // in device memory, declared below, and writes its result into buffers
 // the caller owns.  It calls no cudaMalloc, cudaFree or other allocating
 // routine; the engine's own tables were uploaded when the engine was
@@ -45,6 +45,7 @@
 
 #include "../../include/fk.h"
 #include "fk_internal.h"
+#include "fk_launch.h"
 #include "fk_sieve.cuh"
 
 using namespace fk;
@@ -65,7 +66,14 @@ constexpr size_t kOffXq = 4096;
 constexpr size_t kOffKey = kOffXq + 4ull * kMaxPrimes;
 constexpr size_t kOffCandItem = kOffKey + 8ull * kMaxCand;
 constexpr size_t kOffSort = kOffCandItem + 4ull * kMaxCand;
-constexpr size_t kScratchBytes = kOffSort + 8ull * kMaxCand;
+// ordering: survivors are bucketed by key range (key >> shift, kNaBuckets
+// buckets), scattered into the sort region bucket by bucket, and each
+// bucket is sorted in shared memory by its own CTA
+constexpr uint32_t kNaBuckets = 2048;
+constexpr size_t kOffBucketCnt = kOffSort + 8ull * kMaxCand;
+constexpr size_t kOffBucketStart = kOffBucketCnt + 4ull * kNaBuckets;
+constexpr size_t kOffBucketFill = kOffBucketStart + 4ull * kNaBuckets;
+constexpr size_t kScratchBytes = kOffBucketFill + 4ull * kNaBuckets;
 
 static_assert(sizeof(DevCounters) <= kOffTaskCtr - kOffCtr, "layout");
 static_assert(sizeof(DevItem) <= kOffEngine - kOffItem, "layout");
@@ -85,6 +93,8 @@ T* at(unsigned char* base, size_t off) {
 // counters (the array keeps the last call's contents otherwise).
 __global__ void k_na_init(unsigned char* s, DevEngine eng, DevItem item,
                           unsigned long long ntask) {
+  u32* cnt = reinterpret_cast<u32*>(s + kOffBucketCnt);
+  for (u32 b = threadIdx.x; b < kNaBuckets; b += blockDim.x) cnt[b] = 0u;
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     DevCounters* c = reinterpret_cast<DevCounters*>(s + kOffCtr);
     *c = DevCounters{};
@@ -110,51 +120,148 @@ __global__ void k_na_xq(unsigned char* s) {
   }
 }
 
-// Orders the survivors and writes them, as offsets from the caller's lo,
-// into the caller's buffer (one CTA; bitonic sort inside the array).
-__global__ void __launch_bounds__(kBlock) k_na_finish(
-    unsigned char* s, u64* out, u64 capacity, u64* count, u64 lo_shift) {
+// The call's outcome once the sieve is done: 0 the survivors fit, 1 too
+// many (more than kMaxCand or than the caller's capacity), 2 the pattern
+// staging gave up a bounded wait.
+__device__ __forceinline__ int na_outcome(const unsigned char* s,
+                                          u64 capacity) {
   const DevCounters* c = reinterpret_cast<const DevCounters*>(s + kOffCtr);
+  if (c->overflow & 4u) return 2;
   const u64 n = c->ncand;
-  if (c->overflow & 4u) {             // staging timeout: not a size issue
-    if (threadIdx.x == 0) *count = ~0ull - 1;
-    return;
-  }
-  if (n > kMaxCand || n > capacity || (c->overflow & 1u)) {
-    if (threadIdx.x == 0) *count = ~0ull;
-    return;
-  }
+  if (n > kMaxCand || n > capacity || (c->overflow & 1u)) return 1;
+  return 0;
+}
+
+// Survivors per bucket: bucket (key - lo_shift) >> shift, i.e. by the
+// offset from the caller's lo.
+__global__ void __launch_bounds__(kBlock) k_na_count(unsigned char* s,
+                                                     u64 capacity, u64 lo_shift,
+                                                     u32 shift) {
+  if (na_outcome(s, capacity)) return;
+  const u64 n = reinterpret_cast<const DevCounters*>(s + kOffCtr)->ncand;
   const u64* key = reinterpret_cast<const u64*>(s + kOffKey);
-  u64* buf = reinterpret_cast<u64*>(s + kOffSort);
-  u32 npow = 1;
-  while (npow < n) npow <<= 1;
-  for (u32 i = threadIdx.x; i < npow; i += blockDim.x)
-    buf[i] = i < n ? key[i] : ~0ull;
+  u32* cnt = reinterpret_cast<u32*>(s + kOffBucketCnt);
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n;
+       i += (u64)gridDim.x * blockDim.x) {
+    const u64 b = (key[i] - lo_shift) >> shift;
+    atomicAdd(&cnt[b < kNaBuckets ? b : kNaBuckets - 1], 1u);
+  }
+}
+
+// Exclusive scan of the bucket counts (one CTA): each bucket's first slot
+// in the sort region, twice (start, and the fill cursor the scatter
+// advances).
+__global__ void __launch_bounds__(kBlock) k_na_scan(unsigned char* s,
+                                                    u64 capacity) {
+  if (na_outcome(s, capacity)) return;
+  constexpr u32 per = kNaBuckets / kBlock;
+  const u32* cnt = reinterpret_cast<const u32*>(s + kOffBucketCnt);
+  u32* start = reinterpret_cast<u32*>(s + kOffBucketStart);
+  u32* fill = reinterpret_cast<u32*>(s + kOffBucketFill);
+  __shared__ u32 warp_sum[kBlock / 32];
+  const u32 t = threadIdx.x, lane = t & 31, w = t >> 5;
+  u32 local[per];
+  u32 sum = 0;
+#pragma unroll
+  for (u32 k = 0; k < per; ++k) {
+    local[k] = cnt[t * per + k];
+    sum += local[k];
+  }
+  // inclusive scan of the per-thread sums: within the warp, then across
+  u32 inc = sum;
+#pragma unroll
+  for (u32 d = 1; d < 32; d <<= 1) {
+    const u32 o = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= d) inc += o;
+  }
+  if (lane == 31) warp_sum[w] = inc;
   __syncthreads();
-  for (u32 k = 2; k <= npow; k <<= 1) {
+  u32 before = 0;
+  for (u32 k = 0; k < w; ++k) before += warp_sum[k];
+  u32 at = before + inc - sum;
+#pragma unroll
+  for (u32 k = 0; k < per; ++k) {
+    start[t * per + k] = at;
+    fill[t * per + k] = at;
+    at += local[k];
+  }
+}
+
+// Survivor keys into their buckets' slots of the sort region.
+__global__ void __launch_bounds__(kBlock) k_na_scatter(unsigned char* s,
+                                                       u64 capacity,
+                                                       u64 lo_shift,
+                                                       u32 shift) {
+  if (na_outcome(s, capacity)) return;
+  const u64 n = reinterpret_cast<const DevCounters*>(s + kOffCtr)->ncand;
+  const u64* key = reinterpret_cast<const u64*>(s + kOffKey);
+  u32* fill = reinterpret_cast<u32*>(s + kOffBucketFill);
+  u64* buf = reinterpret_cast<u64*>(s + kOffSort);
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n;
+       i += (u64)gridDim.x * blockDim.x) {
+    const u64 k = key[i];
+    const u64 b = (k - lo_shift) >> shift;
+    buf[atomicAdd(&fill[b < kNaBuckets ? b : kNaBuckets - 1], 1u)] = k;
+  }
+}
+
+// Sorts the c keys at `a` ascending, by one CTA (shared or device
+// memory).  A bitonic network in the form whose blocks all sort upward
+// (the first step of each merge compares mirror positions i and
+// i ^ (k - 1)); positions at or past c act as +infinity and their
+// compare-exchanges are skipped, so c need not be a power of two.
+__device__ void na_sort(u64* a, u32 c) {
+  for (u32 k = 2; (k >> 1) < c; k <<= 1) {
     for (u32 j = k >> 1; j > 0; j >>= 1) {
-      for (u32 i = threadIdx.x; i < npow; i += blockDim.x) {
-        const u32 l = i ^ j;
-        if (l > i) {
-          const u64 x = buf[i], y = buf[l];
-          if ((x > y) == ((i & k) == 0)) {
-            buf[i] = y;
-            buf[l] = x;
+      for (u32 i = threadIdx.x; i < c; i += blockDim.x) {
+        if (i & j) continue;
+        const u32 l = j == (k >> 1) ? i ^ (k - 1) : i | j;
+        if (l < c) {
+          const u64 x = a[i], y = a[l];
+          if (x > y) {
+            a[i] = y;
+            a[l] = x;
           }
         }
       }
       __syncthreads();
     }
   }
-  for (u32 i = threadIdx.x; i < n; i += blockDim.x) out[i] = buf[i] - lo_shift;
-  if (threadIdx.x == 0) *count = n;
 }
 
-template <int P0>
-cudaError_t set_smem_limit() {
-  return cudaFuncSetAttribute(k_sieve<P0>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)(pat_bytes<P0>() + sizeof(SieveSmem)));
+// One CTA per bucket: the bucket's keys sorted in shared memory (in place
+// in the sort region when the bucket outgrows the tile) and written, as
+// offsets from the caller's lo, to the caller's buffer at the bucket's
+// start.  Buckets hold disjoint, increasing key ranges, so the
+// concatenation is the sorted stream.
+__global__ void __launch_bounds__(kBlock) k_na_finish(
+    unsigned char* s, u64* out, u64 capacity, u64* count, u64 lo_shift) {
+  const int outcome = na_outcome(s, capacity);
+  if (outcome) {
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+      *count = outcome == 2 ? ~0ull - 1 : ~0ull;
+    return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    *count = reinterpret_cast<const DevCounters*>(s + kOffCtr)->ncand;
+  u64* buf = reinterpret_cast<u64*>(s + kOffSort);
+  __shared__ u64 tile[kSortSmem];
+  for (u32 b = blockIdx.x; b < kNaBuckets; b += gridDim.x) {
+    const u32 c = reinterpret_cast<const u32*>(s + kOffBucketCnt)[b];
+    if (c == 0) continue;
+    const u32 at0 = reinterpret_cast<const u32*>(s + kOffBucketStart)[b];
+    u64* a = tile;
+    if (c <= (u32)kSortSmem) {
+      for (u32 i = threadIdx.x; i < c; i += blockDim.x) tile[i] = buf[at0 + i];
+    } else {
+      a = buf + at0;
+    }
+    __syncthreads();
+    na_sort(a, c);
+    for (u32 i = threadIdx.x; i < c; i += blockDim.x)
+      out[at0 + i] = a[i] - lo_shift;
+    __syncthreads();
+  }
 }
 
 }  // namespace
@@ -202,9 +309,8 @@ extern "C" fk_status fk_sieve_noalloc(fk_engine* e, const uint64_t lo[2],
       ce = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (ce != cudaSuccess)
         return set_error(FK_ERR_DEVICE, cudaGetErrorString(ce));
-      for (cudaError_t r : {set_smem_limit<7>(), set_smem_limit<6>(),
-                            set_smem_limit<9>(), set_smem_limit<11>()})
-        if (r != cudaSuccess) return set_error(FK_ERR_DEVICE, cudaGetErrorString(r));
+      const cudaError_t r = sieve_set_smem_limits();
+      if (r != cudaSuccess) return set_error(FK_ERR_DEVICE, cudaGetErrorString(r));
       g_scratch_addr[dev] = static_cast<unsigned char*>(p);
     }
     base = g_scratch_addr[dev];
@@ -234,7 +340,7 @@ extern "C" fk_status fk_sieve_noalloc(fk_engine* e, const uint64_t lo[2],
   it.xq_off = 0;
   it.marked = 0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  k_na_init<<<1, 32, 0, s>>>(base, v.dev, it, ntask);
+  k_na_init<<<1, kBlock, 0, s>>>(base, v.dev, it, ntask);
   k_na_xq<<<64, kBlock, 0, s>>>(base);
   SieveArgs a{};
   a.engines = at<DevEngine>(base, kOffEngine);
@@ -252,16 +358,23 @@ extern "C" fk_status fk_sieve_noalloc(fk_engine* e, const uint64_t lo[2],
   a.warp_queue = kWarpMode;
   a.seg_per_task = kSegPerTask;
   const u32 grid = (u32)(ntask < (u64)nsm * 2 ? ntask : (u64)nsm * 2);
-  switch (v.P0) {
-    case 7: k_sieve<7><<<grid, kBlock, pat_bytes<7>() + sizeof(SieveSmem), s>>>(a); break;
-    case 6: k_sieve<6><<<grid, kBlock, pat_bytes<6>() + sizeof(SieveSmem), s>>>(a); break;
-    case 9: k_sieve<9><<<grid, kBlock, pat_bytes<9>() + sizeof(SieveSmem), s>>>(a); break;
-    default: k_sieve<11><<<grid, kBlock, pat_bytes<11>() + sizeof(SieveSmem), s>>>(a); break;
-  }
+  // the engine's own descriptor is the default variant: kNS pattern primes
+  ce = launch_sieve(v.P0, kNS, grid, s, a);
+  if (ce != cudaSuccess) return set_error(FK_ERR_DEVICE, cudaGetErrorString(ce));
   const u64 lo_shift = (u64)(L0 - X0);
-  k_na_finish<<<1, kBlock, 0, s>>>(base, reinterpret_cast<u64*>(d_offsets),
-                                   capacity, reinterpret_cast<u64*>(d_count),
-                                   lo_shift);
+  // bucket = (key - lo_shift) >> shift over the interval's length: at
+  // most kNaBuckets buckets, spread evenly over [lo, hi)
+  const u64 span = (u64)(H0 - L0);
+  u32 shift = 0;
+  while (((span - 1) >> shift) >= kNaBuckets) ++shift;
+  const u32 sgrid = (u32)nsm * 2;
+  k_na_count<<<sgrid, kBlock, 0, s>>>(base, capacity, lo_shift, shift);
+  k_na_scan<<<1, kBlock, 0, s>>>(base, capacity);
+  k_na_scatter<<<sgrid, kBlock, 0, s>>>(base, capacity, lo_shift, shift);
+  k_na_finish<<<sgrid, kBlock, 0, s>>>(base, reinterpret_cast<u64*>(d_offsets),
+                                       capacity,
+                                       reinterpret_cast<u64*>(d_count),
+                                       lo_shift);
   ce = cudaGetLastError();
   if (ce != cudaSuccess) return set_error(FK_ERR_DEVICE, cudaGetErrorString(ce));
   return FK_OK;

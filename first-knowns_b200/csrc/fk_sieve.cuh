@@ -10,7 +10,8 @@
 // items of uneven length run in one launch.
 //
 // S1 (pattern sieve).  For the NS pattern primes starting at prime index
-// P0 -- compile-time constants, so each prime's modulus, word step and
+// P0 (NS = 24, 32 or 40: a template variant chosen per batch) --
+// compile-time constants, so each prime's modulus, word step and
 // table offset are immediates -- the kill pattern of 64 consecutive
 // periods of a lane is one 64-bit word of a per-prime table of q words,
 // indexed by the lane's rotating phase rho (u + s_l) mod q.  The tables
@@ -210,7 +211,7 @@ struct SieveSmem {
   u64 chain_w0[kBlock];   // the thread's first word; word j is w0 + j*stride
   u32 stride;             // 1, or 32 when a warp sweeps one lane
   u32 warp[kBlock / 32];
-  u32 minv[kNS];
+  u32 minv[kNSMax];
   u32 sbits[512];
   u64 task;
   u32 item;
@@ -220,9 +221,11 @@ struct SieveSmem {
   unsigned long long mbar;
 };
 
-template <int P0>
+// Shared bytes of the first NS pattern primes' tables (the prefix a kernel
+// variant stages), padded to 16 bytes.
+template <int P0, int NS = kNS>
 __host__ __device__ constexpr u32 pat_bytes() {
-  return ((fk_pat_prefix(P0, kNS) + 1) / 2) * 16;  // padded to 16 bytes
+  return ((fk_pat_prefix(P0, NS) + 1) / 2) * 16;
 }
 
 // A queued candidate: the chain (thread of the CTA), the word within the
@@ -389,14 +392,15 @@ __device__ __forceinline__ bool mbar_wait(u32 mb, u32 phase, u32 spins) {
   return done != 0;
 }
 
-// Stage an engine's pattern table into shared memory with one bulk async
+// Stage the first NS primes' pattern tables of an engine (a prefix of its
+// table) into shared memory with one bulk async
 // copy (TMA) completing on the CTA's mbarrier, waiting a bounded number of
 // polls.  On a timeout it flags the counters (the host reports
 // FK_ERR_TIMEOUT) and returns false, after a second bounded wait for the
 // copy to land: the CTA then exits, and a copy still writing into the
 // shared memory of an exited CTA is what the second wait avoids.  Every
 // thread of the CTA calls it.
-template <int P0>
+template <int P0, int NS>
 __device__ __forceinline__ bool stage_patterns(u64* spat, const DevEngine& eg,
                                                unsigned long long* mbar,
                                                u32* status, u32& phase,
@@ -405,7 +409,7 @@ __device__ __forceinline__ bool stage_patterns(u64* spat, const DevEngine& eg,
   if (threadIdx.x == 0) {
     *status = 0;
     const u32 mb = smem_u32(mbar);
-    const u32 bytes = pat_bytes<P0>();
+    const u32 bytes = pat_bytes<P0, NS>();
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile(
         "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb),
@@ -427,11 +431,13 @@ __device__ __forceinline__ bool stage_patterns(u64* spat, const DevEngine& eg,
   return *status == 0;
 }
 
-template <int P0>
+// NS: the pattern primes this variant stages (the engine descriptor's NS
+// and round cuts must match it).
+template <int P0, int NS>
 __global__ void __launch_bounds__(kBlock, 3) k_sieve(SieveArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   u64* spat = reinterpret_cast<u64*>(smem_raw);
-  SieveSmem& S = *reinterpret_cast<SieveSmem*>(smem_raw + pat_bytes<P0>());
+  SieveSmem& S = *reinterpret_cast<SieveSmem*>(smem_raw + pat_bytes<P0, NS>());
   const int tid = threadIdx.x;
   if (tid == 0) {
     S.eng = 0xFFFFFFFFu;
@@ -467,9 +473,9 @@ __global__ void __launch_bounds__(kBlock, 3) k_sieve(SieveArgs a) {
     const DevEngine& eg = a.engines[eidx];
     // ---- engine switch: stage its pattern table into shared memory ----
     if (S.eng != eidx) {
-      if (!stage_patterns<P0>(spat, eg, &S.mbar, &S.status, phase, a.ctr))
+      if (!stage_patterns<P0, NS>(spat, eg, &S.mbar, &S.status, phase, a.ctr))
         return;
-      for (u32 i = tid; i < kNS; i += kBlock) S.minv[i] = eg.pat_minv[i];
+      for (u32 i = tid; i < (u32)NS; i += kBlock) S.minv[i] = eg.pat_minv[i];
       for (u32 i = tid; i < eg.sbits_words && i < 512; i += kBlock)
         S.sbits[i] = eg.sbits[i];
       __syncthreads();
@@ -496,8 +502,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_sieve(SieveArgs a) {
     S.chain_R[tid] = R;
     S.chain_w0[tid] = w0;
     if (tid == 0) S.stride = stride;
-    u32 rho[kNS];
-    Pat<P0, 0, kNS>::setup(rho, R, 64ull * w0, a.xq + it.xq_off, S.minv);
+    u32 rho[NS];
+    Pat<P0, 0, NS>::setup(rho, R, 64ull * w0, a.xq + it.xq_off, S.minv);
     const u64 U = it.U;
     u32* wq = S.qa + wid * kWq;
     u32* wq2 = S.qb + wid * kWq;
@@ -519,11 +525,11 @@ __global__ void __launch_bounds__(kBlock, 3) k_sieve(SieveArgs a) {
       if (active) {
         u64 acc[4] = {0, 0, 0, 0};
         if (G == 32)
-          Pat<P0, 0, kNS>::template word2<32>(spat, rho, acc);
+          Pat<P0, 0, NS>::template word2<32>(spat, rho, acc);
         else if (G == 8)
-          Pat<P0, 0, kNS>::template word2<8>(spat, rho, acc);
+          Pat<P0, 0, NS>::template word2<8>(spat, rho, acc);
         else
-          Pat<P0, 0, kNS>::template word2<1>(spat, rho, acc);
+          Pat<P0, 0, NS>::template word2<1>(spat, rho, acc);
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
           const u64 w = w0 + (u64)(wi + k) * stride;

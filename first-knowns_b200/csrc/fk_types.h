@@ -22,7 +22,11 @@ struct PrimeRec {
 
 constexpr int kBlock = 256;       // threads per CTA, every kernel
 constexpr int kQcap = 4096;       // candidate queue entries per CTA (8 warps)
-constexpr int kNS = 32;           // pattern primes per chain
+constexpr int kNS = 32;           // pattern primes per CTA (default)
+constexpr int kNSMin = 24;        // fewest pattern primes a kernel variant
+                                  // stages; marking tables start here
+constexpr int kNSMax = 40;        // most: the engine's pattern tables hold
+                                  // this many primes
 constexpr int kMaxRounds = 64;
 constexpr int kSortSmem = 4096;   // entries a CTA sorts in shared memory
 constexpr int kClassChunk = 128;  // candidates a warp fetches at once
@@ -30,15 +34,21 @@ constexpr int kBucketFill = 1024; // expected entries per ordering bucket
 constexpr int kWarpMode = 32;     // warp queue below which a candidate
                                   // takes a whole warp
 constexpr int kSeg = 32768;       // marking: periods per shared segment
+                                  // (default; variants 16384 and 65536)
+constexpr int kNumSeg = 3;        // marking segment variants
+constexpr int kSegOf(int i) { return 16384 << i; }
 constexpr int kSegPerTask = 8;    // marking: segments per task
-constexpr int kMarkPrimes = 6528; // marking: most primes one engine marks
+constexpr int kMarkPrimes = 6528; // marking: most primes one engine marks,
+                                  // counted from pattern prime kNSMin
                                   // (every prime from 7 to 2^16 fits)
-constexpr int kMarkHits = 16;     // marking: least hits per work entry
+constexpr int kMarkHits = 16;     // marking: least hits per residue of a
+                                  // work entry
 
 // Immutable per-engine tables (device-resident for the engine's life).
 struct DevEngine {
   uint32_t kind, n, L, NP;        // NP: sieve primes (pattern + per-candidate)
-  uint32_t P0, NS, nrounds, xxmax;
+  uint32_t P0, NS, nrounds, xxmax;  // NS: pattern primes of this batch's
+                                    // kernel variant (kNSMin..kNSMax)
   uint32_t pat_words, sbits_words, two_pass, pad0;
   uint64_t M;                     // wheel period (x units)
   uint64_t W;                     // Dickson: k = W * j
@@ -48,8 +58,8 @@ struct DevEngine {
   // entry k = the kill mask of the 64 periods from phase 64k mod q, so
   // consecutive words of a lane are consecutive entries
   const uint64_t* pat;
-  const uint32_t* pat_minv;       // [NS] (M mod q)^-1 * 64^-1 mod q
-  const uint32_t* pat_i64;        // [NS] 64^-1 mod q
+  const uint32_t* pat_minv;       // [kNSMax] (M mod q)^-1 * 64^-1 mod q
+  const uint32_t* pat_i64;        // [kNSMax] 64^-1 mod q
   const PrimeRec* recs;           // [NP]
   const uint32_t* c64;            // [NP] 2^64 mod q
   const uint32_t* lists;          // explicit forbidden-residue lists
@@ -65,14 +75,22 @@ struct DevEngine {
   const uint32_t* minv_all;       // [NP] (M mod q)^-1 mod q
   const uint32_t* gaux;           // [NP] offset | count << 24 into glist
   const uint32_t* glist;
-  // [NPm - NS] per marked prime: q | (kSeg mod q) << 16 | S << 32, where
-  // S is the length of one work entry's sub-range (a multiple of q; 0 when
-  // one entry covers the whole segment)
+  // tables of this batch's segment length SEG (one set per variant):
+  // [NPm - kNSMin] per prime from index kNSMin: q | (SEG mod q) << 16
   const uint64_t* mq;
-  // [nmitems] work entries g | (prime - NS) << 16 | sub-range k << 29 |
-  // q << 32 | S << 48: the hits u = g (mod q), shifted by the lane, inside
-  // sub-range k of length S (one load per entry: q and S ride along)
-  const uint64_t* mitems;
+  // [nmitems] work entries, one per (marked prime, sub-range), four u32
+  // words (16-byte aligned, read as one 16-byte load):
+  //   [0] = (prime - kNSMin) | sub-range k << 13
+  //   [1] = q | S << 16   (S: sub-range length, a multiple of q; 0 when
+  //                        one entry covers the whole segment)
+  //   [2] = first 4-residue slot in mres | residue count << 24, [3] = 0
+  // the entry marks the hits u = g (mod q), shifted by the lane, of every
+  // forbidden period residue g of its prime inside its sub-range; the
+  // batch's pointer starts at the first prime past its pattern primes
+  const uint32_t* mitems;
+  // forbidden period residues per marked prime, u16, each prime's list
+  // padded with 0xFFFF to a multiple of four (one 8-byte load per four)
+  const uint16_t* mres;
 };
 
 // One unit of work: a sub-range of one engine's line.

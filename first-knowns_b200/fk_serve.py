@@ -26,9 +26,17 @@ sieve primes) -- and a batch admits chunks while the sum stays under
 Results are bit-identical to sweeping each request alone with the plain
 engine: every chunk is an independent interval, and a request's chunks
 tile it (the tests check alone == in the mix == plain).
+
+While the loop runs, everything the process built before it (engine
+tables, the caller's objects, imported modules) is moved out of the
+cyclic garbage collector's reach (``gc.freeze``), so a full collection
+triggered by the loop's own small allocations does not rescan that heap
+between two batches: in a process that imports torch such a pass stalls
+the loop for tens to hundreds of milliseconds.
 """
 
 import collections
+import gc
 import time
 
 import numpy as np
@@ -89,6 +97,14 @@ class ServeLoop:
             self._engine(iv)                    # tables resident up front
         for s in self.slots:
             s._ensure()
+        gc.collect()
+        gc.freeze()
+        try:
+            return self._run(requests, time_limit)
+        finally:
+            gc.unfreeze()
+
+    def _run(self, requests, time_limit):
         n = len(requests)
         parts = [None] * n                      # per request: chunk results
         left = [0] * n                          # chunks still out

@@ -3,13 +3,17 @@
 The search space is fk_tuning (include/fk.h): CTAs per SM of the three
 persistent grids (pattern sieve + rounds, marking sieve, SPRP), chains per
 SM when lanes are cut into chains, the compaction cadence (a warp's queue
-shorter than ``warp_queue`` goes one candidate per warp), the marking task length in
-32768-period segments, the lane length from which a warp sweeps one lane,
+shorter than ``warp_queue`` goes one candidate per warp), the marking task
+length in segments, the lane length from which a warp sweeps one lane,
 the lane length from which eight threads sweep one lane
 (``group_lane_words``), the marking sieve's prime bound (primes below
 ``mark_limit`` are marked, the rest tested per candidate), the bias
-between marking and compaction rounds, and the survival at which a
-compaction round is cut (``round_cut``: lower means fewer, longer rounds).
+between marking and compaction rounds, the survival at which a
+compaction round is cut (``round_cut``: lower means fewer, longer rounds),
+and three kernel-variant choices: the marking segment length in bytes
+(``mark_segment``: 16, 32 or 64 KiB of shared byte map) and the pattern
+primes each CTA stages in shared memory, per sieve kernel
+(``pattern_primes``, ``mark_pattern_primes``: 24, 32 or 40).
 None of them can change a result; they only move time.
 
 ``tune`` runs coordinate descent: starting from the current setting it
@@ -37,6 +41,9 @@ SPACE = {
     "warp_lane_words": [64, 1024, 1 << 30],
     "round_cut": [0.3, 0.7, 0.85],
     "group_lane_words": [16, 64, 1 << 30],
+    "pattern_primes": [24, 40],
+    "mark_pattern_primes": [24, 40],
+    "mark_segment": [16384, 65536],
 }
 
 DEFAULT_PATH = pathlib.Path(__file__).resolve().parent / "tuning.json"

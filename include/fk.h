@@ -163,8 +163,7 @@ typedef struct fk_tuning {
   uint32_t warp_queue;           /* compaction: a warp's queue shorter than    *
                                   * this runs one candidate per warp over all  *
                                   * later primes (1-513; 513: always)         */
-  uint32_t seg_per_task;         /* marking: 32768-period segments per task    *
-                                  * (1-64)                                     */
+  uint32_t seg_per_task;         /* marking: segments per task (1-64)          */
   uint32_t classify_ctas_per_sm; /* k_classify grid: CTAs per SM (1-32)        */
   uint32_t mark_limit;           /* sieve-prime bound of the marking sieve:    *
                                   * primes below it are marked, the rest are   *
@@ -183,6 +182,16 @@ typedef struct fk_tuning {
   uint32_t group_lane_words;     /* lanes of at least this many words (and    *
                                   * fewer than warp_lane_words) are swept by  *
                                   * eight threads per lane (>= 8)             */
+  uint32_t mark_segment;         /* marking: periods per shared-memory        *
+                                  * segment, one byte each (16384, 32768 or   *
+                                  * 65536: a kernel variant)                  */
+  uint32_t pattern_primes;       /* pattern sieve + compaction rounds: sieve  *
+                                  * primes each CTA stages as shared-memory   *
+                                  * pattern tables (24, 32 or 40: a kernel    *
+                                  * variant); the rest are tested per         *
+                                  * candidate                                 */
+  uint32_t mark_pattern_primes;  /* the same for the marking sieve (24, 32 or *
+                                  * 40); the primes past them are marked      */
 } fk_tuning;
 fk_status fk_batch_set_tuning(fk_batch* b, const fk_tuning* t);
 fk_status fk_batch_get_tuning(const fk_batch* b, fk_tuning* out);

@@ -155,11 +155,24 @@ def test_tuning_changes_no_result():
                 dict(group_lane_words=8, warp_lane_words=1 << 30),
                 dict(round_cut=0.7), dict(round_cut=0.2, warp_queue=64),
                 dict(round_cut=0.95, mark_bias=0.5),
+                # kernel variants: pattern primes per CTA x marking segment
+                dict(pattern_primes=24, mark_pattern_primes=24,
+                     mark_segment=16384, mark_bias=4.0),
+                dict(pattern_primes=40, mark_pattern_primes=40,
+                     mark_segment=65536, mark_bias=4.0),
+                dict(pattern_primes=24, mark_pattern_primes=40,
+                     mark_segment=16384, mark_limit=4096, seg_per_task=3),
+                dict(pattern_primes=40, mark_pattern_primes=24,
+                     mark_segment=65536, mark_bias=0.25),
+                dict(pattern_primes=32, mark_pattern_primes=32,
+                     mark_segment=65536, seg_per_task=1, mark_bias=2.0),
                 dict(sieve_ctas_per_sm=3, mark_ctas_per_sm=3,
                      classify_ctas_per_sm=8, mark_limit=65536,
                      seg_per_task=8, warp_queue=32, mark_bias=1.0,
                      chains_per_sm=2048, warp_lane_words=256,
-                     round_cut=0.5, group_lane_words=32)]
+                     round_cut=0.5, group_lane_words=32,
+                     pattern_primes=32, mark_pattern_primes=32,
+                     mark_segment=32768)]
     for kw in settings:
         be.set_tuning(**kw)
         assert _same(be.run_arrays(ivs, graph=True), ref), kw
@@ -170,6 +183,12 @@ def test_tuning_changes_no_result():
         be.set_tuning(mark_ctas_per_sm=9)
     with pytest.raises(ValueError):
         be.set_tuning(round_cut=0.99)
+    with pytest.raises(ValueError):
+        be.set_tuning(mark_segment=20000)
+    with pytest.raises(ValueError):
+        be.set_tuning(pattern_primes=33)
+    with pytest.raises(ValueError):
+        be.set_tuning(mark_pattern_primes=16)
 
 
 def test_overflow_grows_the_buffers_and_reruns():

@@ -132,3 +132,36 @@ def test_noalloc_rejects_what_does_not_fit():
     # (UINT64_MAX - 1 would mean a device wait gave up)
     assert _call(f, fk_abi, eng, 10 ** 5, 10 ** 9, out, cnt, cap=16) == 0
     assert int(cnt.item()) == -1
+
+
+def test_noalloc_short_sub_period_and_empty_results():
+    """Survivors are ordered by bucketing their offsets from lo over the
+    interval's length (2048 buckets, each sorted by one CTA): intervals
+    shorter than the bucket count (one offset per bucket, then two), one
+    that sits inside a single period of the 23# wheel, and one with no
+    survivors at all give fk_sieve's stream exactly."""
+    import torch
+    fk_abi, f = _bind()
+    out = torch.zeros(CAP, dtype=torch.int64, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    e2 = fk_abi.Engine(fk_abi.EULER, 2, p0=6)
+    e8 = fk_abi.Engine(fk_abi.EULER, 8, p0=9)
+    e17 = fk_abi.Engine(fk_abi.EULER, 17, p0=11)
+    M23 = 223092870
+    base = 25 * M23
+    # survivor counts (a numpy sieve to 65536): 12, 17, 8 and 0
+    cases = [(e2, 10 ** 12 + 7, 10 ** 12 + 7 + 2047, 10),
+             (e2, 10 ** 12, 10 ** 12 + 4095, 15),
+             (e8, base + 12345, base + 12345 + 2 * 10 ** 8, 5),
+             (e17, 10 ** 16, 10 ** 16 + 10 ** 6, 0)]
+    for eng, lo, hi, least in cases:
+        want = eng.sieve(lo, hi)
+        assert want.size >= least
+        if least == 0:
+            assert want.size == 0
+        out.fill_(-1)
+        cnt.fill_(-1)
+        assert _call(f, fk_abi, eng, lo, hi, out, cnt) == 0
+        n = int(cnt.item())
+        assert n == want.size
+        assert np.array_equal(out[:n].cpu().numpy().view(np.uint64), want)
