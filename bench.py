@@ -93,7 +93,23 @@ def parse():
                     help="run one profiling case (PROFILE_CASES) and exit")
     ap.add_argument("--runs", type=int, default=2,
                     help="--profile-case: runs (the first is a warm-up)")
+    ap.add_argument("--set", action="append", default=[],
+                    metavar="FIELD=VALUE",
+                    help="--profile-case: an fk_tuning field to set "
+                         "(repeatable), e.g. --set mark_segment=65536")
     return ap.parse_args()
+
+
+def tuning_overrides(pairs):
+    """{field: value} from FIELD=VALUE strings (fk_tuning field names)."""
+    import fk_abi
+    out = {}
+    for p in pairs:
+        k, _, v = p.partition("=")
+        if k not in fk_abi.TUNING_FIELDS:
+            raise SystemExit(f"unknown fk_tuning field {k}")
+        out[k] = float(v) if k in fk_abi._FLOAT_FIELDS else int(v)
+    return out
 
 
 # ------------------------------------------------------- profiling cases ---
@@ -116,6 +132,8 @@ PROFILE_CASES = {
     "euler_wide17": "the Euler n = 17 stream over [6.11e20, +2e15) through "
                     "the reference-API mirror (31# wheel; the SCORE_WIDE "
                     "window at a tenth of its length)",
+    "score_wide": "the SCORE_WIDE window itself, [6.11e20, +2e16), through "
+                  "the mirror (one lane per warp: 1563-word lanes)",
 }
 
 
@@ -167,23 +185,29 @@ def profile_intervals(name):
                      f"{', '.join(PROFILE_CASES)}")
 
 
-def run_profile_case(name, runs):
-    if name == "euler_wide17":
+def run_profile_case(name, runs, overrides=None):
+    overrides = overrides or {}
+    if name in ("euler_wide17", "score_wide"):
         from euler_gpu import GpuEngine
         eng = GpuEngine(17)
-        lo, span = 611 * 10 ** 18, 2 * 10 ** 15
+        lo = 611 * 10 ** 18
+        span = 2 * 10 ** (15 if name == "euler_wide17" else 16)
+        if overrides:
+            eng._eng_for(lo, lo + span).set_tuning(**overrides)
         for r in range(runs):
             t0 = time.perf_counter()
             s = eng.survivors_pre_mr(lo, lo + span)
             dt = time.perf_counter() - t0
             st = eng._eng_for(lo, lo + span).stats()
-            print(f"euler_wide17 run {r}: {dt * 1e3:.1f} ms wall, sieve "
+            print(f"{name} run {r}: {dt * 1e3:.1f} ms wall, sieve "
                   f"{st['sieve_ms']:.1f} ms, {len(s)} survivors, s1_words "
                   f"{st['s1_words']}, s2_tests {st['s2_tests']}", flush=True)
         return 0
     from fk_batch import BatchEngine
     ivs = profile_intervals(name)
     be = BatchEngine(ivs)
+    if overrides:
+        be.set_tuning(**overrides)
     for r in range(runs):
         t0 = time.perf_counter()
         rows = be.run_arrays(ivs, graph=False)
@@ -435,7 +459,8 @@ def serve_bench(args):
                "throughput": float(lens[done].sum() / st["wall_s"]),
                "unit": UNIT, "batches": st["batches"],
                "inflight_frac": st["inflight_s"] / st["wall_s"],
-               "device_time_frac": st["device_busy_s"] / st["wall_s"]}
+               "device_time_frac": st["device_busy_s"] / st["wall_s"],
+               "slowest_host_calls": st["slowest_host_calls"]}
         classes = {}
         for name, lo, hi in (("short <2^22", 0, 2 ** 22),
                              ("mid 2^22-2^28", 2 ** 22, 2 ** 28),
@@ -763,7 +788,8 @@ def bench_fk(args):
 def main():
     args = parse()
     if args.profile_case:
-        return run_profile_case(args.profile_case, args.runs)
+        return run_profile_case(args.profile_case, args.runs,
+                                tuning_overrides(args.set))
     if args.impl == "reference":
         return bench_reference(args)
     return bench_fk(args)

@@ -140,9 +140,8 @@ struct fk_engine {
   // per segment length (index seg_index(SEG)): marking work entries before
   // each prime from index kNSMin, and the device tables (mq, mitems)
   std::vector<u32> mprefix[kNumSeg];
-  std::vector<u64> mresidues[kNumSeg];  // residue walks before each prime
   const uint64_t* d_mq[kNumSeg] = {};
-  const uint32_t* d_mitems[kNumSeg] = {};
+  const uint64_t* d_mitems[kNumSeg] = {};
   Cost cost;                  // cost model with every prime below 2^16 marked
   DevEngine dev{};
   std::vector<void*> allocs;
@@ -260,14 +259,11 @@ static Cost engine_cost(const fk_engine* e, u32 NPm, u32 ns_sieve, u32 ns,
   }
   const double npm = NPm > ns ? NPm - ns : 0;
   const std::vector<u32>& mp = e->mprefix[seg_index(seg)];
-  const std::vector<u64>& mr = e->mresidues[seg_index(seg)];
   const double items = NPm > ns && !mp.empty()
                            ? (double)mp[NPm - kNSMin] - mp[ns - kNSMin] : 0;
-  const double walks = NPm > ns && !mr.empty()
-                           ? (double)mr[NPm - kNSMin] - mr[ns - kNSMin] : 0;
   c.round = 2.5 + 22.0 * s1r * tests;
   c.bit = 2.5 + 2.0 + 1.5 * mark_bit + 22.0 * s1 * tail;
-  c.seg = 16.0 * items + 8.0 * walks + 6.0 * npm + 2048.0 * seg / 32768.0;
+  c.seg = 12.0 * items + 6.0 * npm + 2048.0 * seg / 32768.0;
   c.lane = 25.0 * npm;
   c.mark = NPm > ns;
   return c;
@@ -312,8 +308,17 @@ static void set_mark_tables(const fk_engine* e, DevEngine& d, u32 ns,
   d.NS = ns;
   d.NPm = npm;
   d.mq = e->d_mq[si];
-  d.mitems = e->d_mitems[si] + 4 * (npm > ns ? mp[ns - kNSMin] : 0);
-  d.nmitems = npm > ns ? mp[npm - kNSMin] - mp[ns - kNSMin] : 0;
+  const u32 first = npm > ns ? mp[ns - kNSMin] : 0;
+  d.mitems = e->d_mitems[si] + first;
+  d.nmitems = npm > ns ? mp[npm - kNSMin] - first : 0;
+  // the hit classes: primes from q >= seg / 2 on hit a segment at most
+  // twice per residue, from q >= seg on at most once
+  u32 p2 = ns, p1 = ns;
+  while (p2 < npm && e->sieve[p2] < seg / 2) ++p2;
+  p1 = p2;
+  while (p1 < npm && e->sieve[p1] < seg) ++p1;
+  d.nm2 = npm > ns ? mp[p2 - kNSMin] - first : 0;
+  d.nm1 = npm > ns ? mp[p1 - kNSMin] - first : 0;
 }
 
 static fk_status build_engine(fk_engine* e) {
@@ -493,30 +498,15 @@ static fk_status build_engine(fk_engine* e) {
     glist.insert(glist.end(), g.begin(), g.end());
   }
   if (glist.size() >= (1u << 24)) return set_err(FK_ERR_DOMAIN, "glist too large");
-  // ---- marking residue lists: each marked prime's forbidden period
-  // residues as u16, padded to a multiple of four (one 8-byte load each)
-  std::vector<uint16_t> mres;
-  std::vector<u32> mres_at(NP, 0);
-  for (u32 i = kNSMin; i < NPm; ++i) {
-    mres_at[i] = (u32)mres.size();
-    const u32 go = gaux[i] & 0x00FFFFFFu, gc = gaux[i] >> 24;
-    for (u32 c = 0; c < gc; ++c) mres.push_back((uint16_t)glist[go + c]);
-    while (mres.size() % 4) mres.push_back(0xFFFFu);
-  }
-  if (mres.size() >= (1u << 26)) return set_err(FK_ERR_DOMAIN, "mres too large");
-  // ---- marking work lists, one per segment length SEG: one entry per
-  // (prime, sub-range) from prime index kNSMin, each walking all of its
-  // prime's residues; small primes are cut into sub-ranges of at least
-  // kMarkHits hits per residue and at most 8 per segment, so the heavy
-  // primes spread over the threads.  Ordered by prime: a warp's entries
-  // share q, residue count and trip counts.
+  // ---- marking work lists, one per segment length SEG: every (prime,
+  // forbidden residue) progression from prime index kNSMin, cut into
+  // sub-ranges of at least kMarkHits hits and at most 8 per segment,
+  // ordered by prime so a warp's entries share q and trip counts
   std::vector<u64> mq[kNumSeg];
-  std::vector<u32> mitems[kNumSeg];   // four words per entry
+  std::vector<u64> mitems[kNumSeg];
   for (int si = 0; si < kNumSeg; ++si) {
     const u32 seg = (u32)kSegOf(si);
     e->mprefix[si].clear();
-    e->mresidues[si].clear();
-    u64 nres = 0;
     for (u32 i = kNSMin; i < NPm; ++i) {
       const u32 q = e->sieve[i];
       const u32 pi = i - kNSMin;
@@ -527,20 +517,14 @@ static fk_status build_engine(fk_engine* e) {
         nsub = (seg + S - 1) / S;
       }
       mq[si].push_back((u64)q | ((u64)(seg % q) << 16));
-      e->mprefix[si].push_back((u32)(mitems[si].size() / 4));
-      e->mresidues[si].push_back(nres);
-      const u32 gc = gaux[i] >> 24;
-      if (gc == 0) continue;
-      for (u32 k = 0; k < nsub; ++k) {
-        mitems[si].push_back(pi | (k << 13));
-        mitems[si].push_back(q | (S << 16));
-        mitems[si].push_back((mres_at[i] / 4) | (gc << 24));
-        mitems[si].push_back(0);
-        nres += gc;
-      }
+      e->mprefix[si].push_back((u32)mitems[si].size());
+      const u32 go = gaux[i] & 0x00FFFFFFu, gc = gaux[i] >> 24;
+      for (u32 k = 0; k < nsub; ++k)
+        for (u32 c = 0; c < gc; ++c)
+          mitems[si].push_back((u64)(glist[go + c] | (pi << 16) | (k << 29)) |
+                               ((u64)q << 32) | ((u64)S << 48));
     }
-    e->mprefix[si].push_back((u32)(mitems[si].size() / 4));
-    e->mresidues[si].push_back(nres);
+    e->mprefix[si].push_back((u32)mitems[si].size());
   }
   e->cost = engine_cost(e, NPm, kNS, kNS, kSeg);
   e->use_mark = e->cost.mark;
@@ -579,7 +563,6 @@ static fk_status build_engine(fk_engine* e) {
   if ((st = upload(e, minv_all, &d.minv_all))) return st;
   if ((st = upload(e, gaux, &d.gaux))) return st;
   if ((st = upload(e, glist, &d.glist))) return st;
-  if ((st = upload(e, mres, &d.mres))) return st;
   for (int si = 0; si < kNumSeg; ++si) {
     if ((st = upload(e, mq[si], &e->d_mq[si]))) return st;
     if ((st = upload(e, mitems[si], &e->d_mitems[si]))) return st;
@@ -591,13 +574,17 @@ static fk_status build_engine(fk_engine* e) {
 }
 
 // ----------------------------------------------------------------- batch ---
+// Device and pinned host buffers grow geometrically (at least 1.5x the
+// old capacity): a stream of batches of slowly rising size then reallocates
+// a logarithmic number of times, since each regrowth frees the old buffer
+// (cudaFree / cudaFreeHost wait for the device) and pins new host pages.
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
   u64 cap = 0;
   fk_status ensure(u64 n) {
     if (n <= cap && p) return FK_OK;
-    u64 c = std::max<u64>(n, 1024);
+    u64 c = std::max<u64>({n, (u64)1024, cap + cap / 2});
     if (p) cudaFree(p);
     p = nullptr;
     cap = 0;
@@ -618,7 +605,7 @@ struct PinBuf {
   u64 cap = 0;
   fk_status ensure(u64 n) {
     if (n <= cap && p) return FK_OK;
-    u64 c = std::max<u64>(n, 1024);
+    u64 c = std::max<u64>({n, (u64)1024, cap + cap / 2});
     if (p) cudaFreeHost(p);
     p = nullptr;
     cap = 0;

@@ -9,15 +9,14 @@
 //   (a) ORs the NS compile-time pattern primes into SEG / 16384 words per
 //       thread (the stage-1a pattern sieve of fk_sieve.cuh),
 //   (b) marks every other prime below 2^16 into a SEG-byte shared map.
-//       A work entry is one prime (or, for the small primes, one
-//       sub-range of at least kMarkHits hits per residue): it sets up the
-//       prime's offset and bounds once and then writes the progression of
-//       step q of each of the prime's forbidden residues.  Entries are
-//       built once per engine and ordered by prime; the threads take them
+//       Each (prime, forbidden residue) progression of step q is one or
+//       more work entries of at least kMarkHits hits (the large primes:
+//       one entry of at most two hits), built once per engine and
+//       segment length and ordered by prime; the threads take the entries
 //       round robin, so the heavy small primes spread over every warp and
-//       a warp's entries share q, residue count and trip counts.  Marks
-//       are plain byte stores (a mark is idempotent: no read-modify-write,
-//       no atomic), four per loop trip, and
+//       a warp's entries share q and trip count.  Marks are plain byte
+//       stores (a mark is idempotent: no read-modify-write, no atomic),
+//       four per loop trip, and
 //   (c) extracts the periods that neither marked, tests any primes beyond
 //       the marked range one by one, and appends the survivors to the
 //       candidate list.
@@ -182,60 +181,76 @@ __global__ void __launch_bounds__(kBlock, 3) k_mark(SieveArgs a) {
     for (u64 useg = u_start; useg < u_end; useg += SEG) {
       const u32 seg_len = (u32)min((u64)SEG, u_end - useg);
       // (a) the pattern words WPT*tid ... WPT*tid + WPT - 1
+      // (a thread whose words all lie past the segment's end skips it:
+      // a short lane's last segment leaves most threads idle)
       u64 acc[WPT];
 #pragma unroll
       for (int k = 0; k < WPT; ++k) acc[k] = 0;
-      PatSeg<P0, 0, NS, WPT>::words(spat, S.ph, (u32)(WPT * tid), acc);
-      nword += WPT;
-      // zero the byte map
+      if (64u * WPT * (u32)tid < seg_len) {
+        PatSeg<P0, 0, NS, WPT>::words(spat, S.ph, (u32)(WPT * tid), acc);
+        nword += WPT;
+      }
+      // zero the byte map up to the segment's end
       {
         uint4* b4 = reinterpret_cast<uint4*>(S.bytes);
         const uint4 z = make_uint4(0, 0, 0, 0);
 #pragma unroll
-        for (int k = 0; k < SEG / 16 / kBlock; ++k) b4[tid + k * kBlock] = z;
+        for (int k = 0; k < SEG / 16 / kBlock; ++k) {
+          const u32 idx = tid + k * kBlock;
+          if (16u * idx < seg_len) b4[idx] = z;
+        }
       }
       __syncthreads();
       // (b) mark: the work entries round robin over the threads, the next
-      // entry's load in flight while this one is walked.  An entry is one
-      // prime's sub-range: its offset and bounds are set up once, then
-      // each forbidden residue's progression is written, four residues
-      // per 8-byte load of the residue list
+      // two entries' loads in flight while this one's progression is
+      // written (an entry carries its prime and sub-range length: one load
+      // each).
+      // Entries come ordered by prime, so a warp's 32 consecutive entries
+      // share a hit class: from index nm2 on, a residue hits the segment
+      // at most twice (q >= SEG / 2), from nm1 on at most once (q >= SEG),
+      // and those are written by a fixed predicated sequence instead of
+      // the loops
       {
-        const u32 nm = e.nmitems;
-        const uint4* __restrict__ mit = reinterpret_cast<const uint4*>(e.mitems);
-        const uint2* __restrict__ mres = reinterpret_cast<const uint2*>(e.mres);
+        const u32 nm = e.nmitems, nm2 = e.nm2, nm1 = e.nm1;
+        const u64* __restrict__ mit = reinterpret_cast<const u64*>(e.mitems);
         unsigned char* __restrict__ B = S.bytes;
         u32 cnt = 0;
         u32 i = tid;
-        uint4 w = i < nm ? __ldg(mit + i) : make_uint4(0, 0, 0, 0);
+        // two entries' loads in flight ahead of the one being written: a
+        // large prime's entry is a handful of instructions, too few to
+        // cover one L2 round trip
+        u64 w = i < nm ? __ldg(mit + i) : 0ull;
+        u64 w1 = i + kBlock < nm ? __ldg(mit + i + kBlock) : 0ull;
         while (i < nm) {
           const u32 inext = i + kBlock;
-          const uint4 wn = inext < nm ? __ldg(mit + inext) : make_uint4(0, 0, 0, 0);
-          const u32 pi = w.x & 0x1FFFu, k = w.x >> 13;
-          const u32 q = w.y & 0xFFFFu, sl = w.y >> 16;
-          const u32 gslot = w.z & 0x00FFFFFFu, gc = w.z >> 24;
+          const u64 wn = w1;
+          w1 = inext + kBlock < nm ? __ldg(mit + inext + kBlock) : 0ull;
+          const u32 wl = (u32)w, wh = (u32)(w >> 32);
+          const u32 g = wl & 0xFFFFu, pi = (wl >> 16) & 0x1FFFu;
+          const u32 q = wh & 0xFFFFu;
           const u32 off = S.off16[pi];
-          const u32 base = k * sl;
-          const u32 end = sl ? min(seg_len, base + sl) : seg_len;
-          const u32 q2 = 2 * q, q3 = 3 * q, q4 = 4 * q;
-          for (u32 c = 0; c < gc; c += 4) {
-            const uint2 gg = __ldg(mres + gslot + (c >> 2));
-            const u32 gv[4] = {gg.x & 0xFFFFu, gg.x >> 16, gg.y & 0xFFFFu,
-                               gg.y >> 16};
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              if (gv[j] == 0xFFFFu) break;   // the list's padding
-              const u32 d = gv[j] - off;
-              u32 h = min(d, d + q) + base;  // (g - off) mod q, then the
-                                             // sub-range's start
-              for (; h + q3 < end; h += q4, cnt += 4) {
-                B[h] = 1;
-                B[h + q] = 1;
-                B[h + q2] = 1;
-                B[h + q3] = 1;
-              }
-              for (; h < end; h += q, ++cnt) B[h] = 1;
+          const u32 d = g - off;
+          u32 h = min(d, d + q);   // (g - off) mod q: the first hit
+          if (i >= nm2) {
+            // whole-segment entries of large primes: h < q, so h + q is
+            // the last possible hit (h + 2q >= 2q >= SEG)
+            if (h < seg_len) { B[h] = 1; ++cnt; }
+            if (i < nm1) {
+              h += q;
+              if (h < seg_len) { B[h] = 1; ++cnt; }
             }
+          } else {
+            const u32 k = wl >> 29, sl = wh >> 16;
+            h += k * sl;
+            const u32 end = sl ? min(seg_len, (k + 1) * sl) : seg_len;
+            const u32 q2 = 2 * q, q3 = 3 * q, q4 = 4 * q;
+            for (; h + q3 < end; h += q4, cnt += 4) {
+              B[h] = 1;
+              B[h + q] = 1;
+              B[h + q2] = 1;
+              B[h + q3] = 1;
+            }
+            for (; h < end; h += q, ++cnt) B[h] = 1;
           }
           i = inext;
           w = wn;

@@ -41,8 +41,7 @@ constexpr int kSegPerTask = 8;    // marking: segments per task
 constexpr int kMarkPrimes = 6528; // marking: most primes one engine marks,
                                   // counted from pattern prime kNSMin
                                   // (every prime from 7 to 2^16 fits)
-constexpr int kMarkHits = 16;     // marking: least hits per residue of a
-                                  // work entry
+constexpr int kMarkHits = 16;     // marking: least hits per work entry
 
 // Immutable per-engine tables (device-resident for the engine's life).
 struct DevEngine {
@@ -71,26 +70,25 @@ struct DevEngine {
   // byte map; G lists hold each prime's forbidden residues of the PERIOD
   // u for lane offset 0 (f * (M mod q)^-1 mod q)
   uint32_t NPm, use_mark;
-  uint32_t nmitems, pad3;         // marking work entries
+  uint32_t nmitems;               // marking work entries of this batch
+  uint32_t nm2, nm1;              // entries before the first prime with
+                                  // q >= SEG / 2 (at most two hits per
+                                  // segment) and with q >= SEG (at most
+                                  // one); both relative to mitems
+  uint32_t pad3;
   const uint32_t* minv_all;       // [NP] (M mod q)^-1 mod q
   const uint32_t* gaux;           // [NP] offset | count << 24 into glist
   const uint32_t* glist;
   // tables of this batch's segment length SEG (one set per variant):
   // [NPm - kNSMin] per prime from index kNSMin: q | (SEG mod q) << 16
   const uint64_t* mq;
-  // [nmitems] work entries, one per (marked prime, sub-range), four u32
-  // words (16-byte aligned, read as one 16-byte load):
-  //   [0] = (prime - kNSMin) | sub-range k << 13
-  //   [1] = q | S << 16   (S: sub-range length, a multiple of q; 0 when
-  //                        one entry covers the whole segment)
-  //   [2] = first 4-residue slot in mres | residue count << 24, [3] = 0
-  // the entry marks the hits u = g (mod q), shifted by the lane, of every
-  // forbidden period residue g of its prime inside its sub-range; the
-  // batch's pointer starts at the first prime past its pattern primes
-  const uint32_t* mitems;
-  // forbidden period residues per marked prime, u16, each prime's list
-  // padded with 0xFFFF to a multiple of four (one 8-byte load per four)
-  const uint16_t* mres;
+  // [nmitems] work entries g | (prime - kNSMin) << 16 | sub-range k << 29 |
+  // q << 32 | S << 48: the hits u = g (mod q), shifted by the lane, of one
+  // forbidden period residue g inside sub-range k of length S (a multiple
+  // of q; S = 0 when the entry covers the whole segment), one 8-byte load
+  // per entry; ordered by prime, and the batch's pointer starts at the
+  // first prime past its pattern primes
+  const uint64_t* mitems;
 };
 
 // One unit of work: a sub-range of one engine's line.

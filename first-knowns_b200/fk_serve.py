@@ -119,6 +119,7 @@ class ServeLoop:
         last = 0.0
         batches = 0
         work_done = 0
+        host_calls = []                         # (host s, kind, t, chunks)
         while nxt < n or queue or inflight:
             now = time.perf_counter() - t0
             if inflight:
@@ -138,7 +139,10 @@ class ServeLoop:
                 if not self.slots[si]._batch.ready():
                     continue
                 done = inflight.pop(si)
+                tw = time.perf_counter()
                 rows = self.slots[si].wait_arrays()
+                host_calls.append((time.perf_counter() - tw, "wait",
+                                   tw - t0, len(done)))
                 st = self.slots[si].stats()
                 busy_s += st["total_ms"] * 1e-3
                 t_done = time.perf_counter() - t0
@@ -169,7 +173,10 @@ class ServeLoop:
                     take.append(queue.popleft())
                     foot += f
                     work += hi - lo
+                ts = time.perf_counter()
                 self.slots[si].submit([c for _, _, c in take])
+                host_calls.append((time.perf_counter() - ts, "submit",
+                                   ts - t0, len(take)))
                 inflight[si] = take
                 batches += 1
                 work_done += work
@@ -181,9 +188,16 @@ class ServeLoop:
                 time.sleep(0.0001)
         wall = time.perf_counter() - t0
         served = ~np.isnan(latency)
+        host_calls.sort(reverse=True)
         stats = {"requests": int(served.sum()), "batches": batches,
                  "wall_s": wall, "device_busy_s": busy_s,
-                 "inflight_s": inflight_s, "line_units": work_done}
+                 "inflight_s": inflight_s, "line_units": work_done,
+                 # the five longest submit / wait calls on the host: a
+                 # stall there holds every queued request
+                 "slowest_host_calls": [
+                     {"ms": round(d * 1e3, 2), "call": k,
+                      "at_s": round(t, 3), "chunks": n}
+                     for d, k, t, n in host_calls[:5]]}
         return results, latency, stats
 
     def _join(self, iv, parts):

@@ -31,7 +31,7 @@ import time
 
 SPACE = {
     "mark_bias": [0.5, 0.7, 1.4, 2.0],
-    "mark_limit": [8192, 16384, 32768, 65536],
+    "mark_limit": [49152, 65536],
     "seg_per_task": [2, 4, 8, 16],
     "chains_per_sm": [1024, 2048, 4096, 8192],
     "warp_queue": [8, 16, 64, 128],
@@ -49,12 +49,16 @@ SPACE = {
 DEFAULT_PATH = pathlib.Path(__file__).resolve().parent / "tuning.json"
 
 
-def measure(engine, intervals, repeats=2):
-    """Median device time (ms) of the batch pipeline on the intervals."""
+def measure(engine, intervals, repeats=2, give_up_ms=None):
+    """Median device time (ms) of the batch pipeline on the intervals.  A
+    first run slower than ``give_up_ms`` is returned alone: a setting that
+    far behind is not timed again."""
     times = []
     for _ in range(repeats):
         engine.run_arrays(intervals, graph=False)
         times.append(engine.stats()["total_ms"])
+        if give_up_ms is not None and times[0] > give_up_ms:
+            return times[0]
     return statistics.median(times)
 
 
@@ -80,7 +84,8 @@ def tune(engine, intervals, repeats=2, max_passes=2, budget_s=120.0,
                 cand = dict(best)
                 cand[key] = v
                 engine.set_tuning(**cand)
-                ms = measure(engine, intervals, repeats)
+                ms = measure(engine, intervals, repeats,
+                             give_up_ms=1.5 * best_ms)
                 trials.append({"setting": cand, "ms": ms})
                 if log:
                     log(f"tune {key}={v}: {ms:.1f} ms (best {best_ms:.1f})")

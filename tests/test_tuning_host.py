@@ -17,7 +17,7 @@ import fk_workloads as W
 
 class FakeBatch:
     """Stands in for BatchEngine: total_ms is a known function of the
-    setting (best at mark_bias 1.4, mark_limit 32768, seg_per_task 4)."""
+    setting (best at mark_bias 1.4, mark_limit 49152, seg_per_task 4)."""
 
     def __init__(self):
         import fk_tune
@@ -39,7 +39,7 @@ class FakeBatch:
         s = self.setting
         ms = 100.0
         ms += 40 * abs(s["mark_bias"] - 1.4)
-        ms += 0.001 * abs(s["mark_limit"] - 32768)
+        ms += 0.001 * abs(s["mark_limit"] - 49152)
         ms += 5 * abs(s["seg_per_task"] - 4)
         return {"total_ms": ms}
 
@@ -50,11 +50,25 @@ def test_coordinate_descent_finds_the_minimum():
     res = fk_tune.tune(fb, [], repeats=1, max_passes=3, budget_s=60)
     best = res["best"]
     assert best["mark_bias"] == 1.4
-    assert best["mark_limit"] == 32768
+    assert best["mark_limit"] == 49152
     assert best["seg_per_task"] == 4
     assert fb.setting == best                   # applied
     assert res["best_ms"] == pytest.approx(100.0)
     assert len(res["trials"]) > 1
+
+
+def test_a_far_slower_setting_is_timed_once():
+    """A candidate whose first run is over 1.5x the incumbent is not run
+    again: the budget goes to settings that can win."""
+    import fk_tune
+    fb = FakeBatch()
+    fb.setting.update(mark_bias=50.0)            # 2000 ms slower
+    ms = fk_tune.measure(fb, [], repeats=3, give_up_ms=150.0)
+    assert fb.runs == 1 and ms > 150.0
+    fb.runs = 0
+    fb.setting.update(mark_bias=1.4)
+    fk_tune.measure(fb, [], repeats=3, give_up_ms=150.0)
+    assert fb.runs == 3
 
 
 def test_tuner_keeps_to_its_budget():
