@@ -690,7 +690,7 @@ static const fk_tuning kDefaultTuning = {3, 3, 2048, (u32)kWarpMode,
                                          (u32)kSegPerTask, 8, 65536, 1.0f,
                                          256, 1.0f,
                                          (float)kDefaultRoundCut, 32,
-                                         (u32)kSeg, (u32)kNS, (u32)kNS};
+                                         (u32)kSeg, (u32)kNS, (u32)kNS, 8};
 
 // Upload this batch's copy of every engine descriptor: the kernel
 // variant's pattern-prime count and segment tables, the marked prime range
@@ -904,7 +904,7 @@ static fk_status expand(fk_batch* b, const fk_item* items, u64 nitems) {
         di.Tc = (u32)tc;
         di.nchunk = (words + G * tc - 1) / (G * tc);
         const u64 chains = di.nchunk * L;      // one per group
-        const u64 per_task = kBlock / G;
+        const u64 per_task = (u64)b->tune.warp_tasks * (32 / G);
         di.ntask = (chains + per_task - 1) / per_task;
       }
       Family& f = b->fam[fam_of(e->P0, mark)];
@@ -1026,6 +1026,7 @@ static fk_status enqueue(fk_batch* b, bool capturing = false) {
     a.task_ctr = b->d_task_ctr.p + f;
     a.warp_queue = b->tune.warp_queue;
     a.seg_per_task = b->tune.seg_per_task;
+    a.warp_tasks = b->tune.warp_tasks;
     const u64 grid = std::min<u64>(
         a.ntask, (u64)b->nsm * (F.mark ? b->tune.mark_ctas_per_sm
                                        : b->tune.sieve_ctas_per_sm));
@@ -1134,7 +1135,7 @@ static fk_status launch(fk_batch* b, int use_graph) {
   key.push_back((u64)(uintptr_t)b->d_cand_key.p);
   key.push_back(((u64)b->tune.sieve_ctas_per_sm << 32) | b->tune.mark_ctas_per_sm);
   key.push_back(((u64)b->tune.warp_queue << 32) | b->tune.seg_per_task);
-  key.push_back(b->tune.classify_ctas_per_sm);
+  key.push_back(((u64)b->tune.warp_tasks << 32) | b->tune.classify_ctas_per_sm);
   key.push_back(((u64)b->tune.pattern_primes << 48) |
                 ((u64)b->tune.mark_pattern_primes << 32) | b->tune.mark_segment);
   if (b->gexec == nullptr || key != b->graph_key) {
@@ -1445,6 +1446,9 @@ fk_status fk_batch_set_tuning(fk_batch* b, const fk_tuning* t) {
   if (t->mark_segment) n.mark_segment = t->mark_segment;
   if (t->pattern_primes) n.pattern_primes = t->pattern_primes;
   if (t->mark_pattern_primes) n.mark_pattern_primes = t->mark_pattern_primes;
+  if (t->warp_tasks) n.warp_tasks = t->warp_tasks;
+  if (n.warp_tasks != 8 && n.warp_tasks != 16 && n.warp_tasks != 32)
+    return set_err(FK_ERR_DOMAIN, "warp_tasks must be 8, 16 or 32");
   if (!valid_mark_segment(n.mark_segment) ||
       !valid_pattern_primes(n.pattern_primes) ||
       !valid_pattern_primes(n.mark_pattern_primes))

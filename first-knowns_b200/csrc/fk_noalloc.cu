@@ -357,6 +357,7 @@ extern "C" fk_status fk_sieve_noalloc(fk_engine* e, const uint64_t lo[2],
   a.task_ctr = at<unsigned long long>(base, kOffTaskCtr);
   a.warp_queue = kWarpMode;
   a.seg_per_task = kSegPerTask;
+  a.warp_tasks = kBlock / 32;  // ntask above counts kBlock chains per task
   const u32 grid = (u32)(ntask < (u64)nsm * 2 ? ntask : (u64)nsm * 2);
   // the engine's own descriptor is the default variant: kNS pattern primes
   ce = launch_sieve(v.P0, kNS, grid, s, a);

@@ -7,7 +7,8 @@
 // on words t, t + 32, ... (so a warp's pattern loads are 32 consecutive
 // table entries).  A CTA runs 256 threads' chains (a TASK), and a
 // persistent grid pulls tasks from a device counter, so thousands of
-// items of uneven length run in one launch.
+// items of uneven length run in one launch.  Inside a task the warps claim
+// blocks of 32 threads' chains (warp tasks) from a shared counter.
 //
 // S1 (pattern sieve).  For the NS pattern primes starting at prime index
 // P0 (NS = 24, 32 or 40: a template variant chosen per batch) --
@@ -181,6 +182,9 @@ struct SieveArgs {
   u32 warp_queue;     // compaction: warp queues below this go one
                       // candidate per warp
   u32 seg_per_task;   // marking: segments per task
+  u32 warp_tasks;     // pattern sieve: warp tasks per CTA task (8, 16 or
+                      // 32); a warp task is one warp's 32 threads' chains
+  u32 pad2;
 };
 
 // The entry of the item holding task t: the last i with task_prefix[i] <=
@@ -210,6 +214,7 @@ struct SieveSmem {
   u64 chain_R[kBlock];
   u64 chain_w0[kBlock];   // the thread's first word; word j is w0 + j*stride
   u32 stride;             // 1, or 32 when a warp sweeps one lane
+  u32 wnext;              // the CTA task's next warp task
   u32 warp[kBlock / 32];
   u32 minv[kNSMax];
   u32 sbits[512];
@@ -257,7 +262,7 @@ __device__ __forceinline__ void emit_cand(const SieveArgs& a, u64 v,
 template <int KIND>
 __device__ void warp_drain(u32* qin, u32* qout, u32 n, const SieveSmem& S,
                            const DevEngine& e, const DevItem& it, u32 gitem,
-                           const SieveArgs& a, u32 wq_short, u64& ntest) {
+                           const SieveArgs& a, u32 wq_short, u32& ntest) {
   const u32 lane = threadIdx.x & 31;
   const u32 lt = (1u << lane) - 1u;
   const u32* __restrict__ xq = a.xq + it.xq_off;
@@ -365,7 +370,7 @@ __device__ __forceinline__ void drain_any(u32* qin, u32* qout, u32 n,
                                           const DevEngine& e,
                                           const DevItem& it, u32 gitem,
                                           const SieveArgs& a, u32 wq_short,
-                                          u64& ntest) {
+                                          u32& ntest) {
   switch (e.kind) {
     case KIND_EULER:
       warp_drain<KIND_EULER>(qin, qout, n, S, e, it, gitem, a, wq_short, ntest);
@@ -454,6 +459,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_sieve(SieveArgs a) {
     if (tid == 0) {
       const u64 t = atomicAdd(a.task_ctr, 1ull);
       S.task = t;
+      S.wnext = 0;
       if (t < a.ntask) {
         // binary search: last entry with task_prefix[i] <= t
         u32 lo = 0, hi = a.nitems;
@@ -462,6 +468,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_sieve(SieveArgs a) {
           if (a.task_prefix[mid] <= t) lo = mid; else hi = mid;
         }
         S.item = lo;
+        S.stride = a.items[a.item_index[lo]].lane_threads;
       }
     }
     __syncthreads();
@@ -482,7 +489,11 @@ __global__ void __launch_bounds__(kBlock, 3) k_sieve(SieveArgs a) {
       if (tid == 0) S.eng = eidx;
     }
     const DevEngine e = eg;
-    // ---- this thread's chain -------------------------------------------
+    // ---- warp tasks ------------------------------------------------------
+    // A CTA task is a.warp_tasks blocks of 32 threads' chains; each warp
+    // claims blocks from the CTA's counter until none is left, so a warp
+    // held up by a long queue drain takes fewer of them and the barrier
+    // that ends the CTA task comes once per a.warp_tasks blocks.
     // G = lane_threads threads sweep one lane: thread t of the group takes
     // words t, t + G, ... of a G * Tc word block, so a group's pattern
     // loads are G consecutive table entries (G = 1: one lane per thread,
@@ -490,110 +501,123 @@ __global__ void __launch_bounds__(kBlock, 3) k_sieve(SieveArgs a) {
     const u32 G = it.lane_threads;
     const u32 gsh = G == 32 ? 5u : (G == 8 ? 3u : 0u);
     const u32 wl = tid & 31, wid = tid >> 5;
-    const u64 g = (task - a.task_prefix[S.item]) * (u64)(kBlock >> gsh) +
-                  (tid >> gsh);
     const u64 nchain = it.nchunk * e.L;
-    const bool active = g < nchain;
-    const u64 chunk = active ? g / e.L : 0;
-    const u32 lane = active ? (u32)(g % e.L) : 0;
-    const u64 R = active ? e.lanes[lane] : 0;
-    const u64 w0 = chunk * (u64)G * it.Tc + (tid & (G - 1));
-    const u32 stride = G;
-    S.chain_R[tid] = R;
-    S.chain_w0[tid] = w0;
-    if (tid == 0) S.stride = stride;
-    u32 rho[NS];
-    Pat<P0, 0, NS>::setup(rho, R, 64ull * w0, a.xq + it.xq_off, S.minv);
+    const u64 wt0 = (task - a.task_prefix[S.item]) * (u64)a.warp_tasks;
+    const u32 cpw = 32u >> gsh;  // chains per warp task
     const u64 U = it.U;
     u32* wq = S.qa + wid * kWq;
     u32* wq2 = S.qb + wid * kWq;
     const u32 wq_short = a.warp_queue;
-    u32 qn = 0;
-    u64 ntest = 0, nword = 0;
+    const u32 stride = G;
     // words below wfull end before the item's last period, so only the
     // first word (lo_off) and the last (hi_last, U) need a validity mask
     const u64 wfull = U ? (U - 1) >> 6 : 0;
-    if (active) {
-      // the chain's words in range: j < Tc with w0 + j*stride < ceil(U/64)
-      const u64 wend = (U + 63) >> 6;
-      if (w0 < wend) nword = min((u64)it.Tc, (wend - w0 + stride - 1) / stride);
-    }
-    __syncthreads();
-    for (u32 wi = 0; wi < it.Tc; wi += 2) {
-      // two words of the chain: j = wi and wi + 1
-      u64 sv[2] = {0, 0};
+    u32 ntest = 0, nword = 0;  // this CTA task's counts
+    for (;;) {
+      u32 wt = 0;
+      if (wl == 0) wt = atomicAdd(&S.wnext, 1u);
+      wt = __shfl_sync(0xffffffffu, wt, 0);
+      if (wt >= a.warp_tasks) break;
+      const u64 gw = (wt0 + wt) * cpw;       // the warp task's first chain
+      if (gw >= nchain) break;               // and every later one's too
+      // ---- this thread's chain -----------------------------------------
+      const u64 g = gw + (wl >> gsh);
+      const bool active = g < nchain;
+      const u64 chunk = active ? g / e.L : 0;
+      const u32 lane = active ? (u32)(g % e.L) : 0;
+      const u64 R = active ? e.lanes[lane] : 0;
+      const u64 w0 = chunk * (u64)G * it.Tc + (wl & (G - 1));
+      S.chain_R[tid] = R;
+      S.chain_w0[tid] = w0;
+      u32 rho[NS];
+      Pat<P0, 0, NS>::setup(rho, R, 64ull * w0, a.xq + it.xq_off, S.minv);
+      u32 qn = 0;
       if (active) {
-        u64 acc[4] = {0, 0, 0, 0};
-        if (G == 32)
-          Pat<P0, 0, NS>::template word2<32>(spat, rho, acc);
-        else if (G == 8)
-          Pat<P0, 0, NS>::template word2<8>(spat, rho, acc);
-        else
-          Pat<P0, 0, NS>::template word2<1>(spat, rho, acc);
+        // the chain's words in range: j < Tc with w0 + j*stride < ceil(U/64)
+        const u64 wend = (U + 63) >> 6;
+        if (w0 < wend)
+          nword += (u32)min((u64)it.Tc, (wend - w0 + stride - 1) / stride);
+      }
+      __syncwarp();
+      for (u32 wi = 0; wi < it.Tc; wi += 2) {
+        // two words of the chain: j = wi and wi + 1
+        u64 sv[2] = {0, 0};
+        if (active) {
+          u64 acc[4] = {0, 0, 0, 0};
+          if (G == 32)
+            Pat<P0, 0, NS>::template word2<32>(spat, rho, acc);
+          else if (G == 8)
+            Pat<P0, 0, NS>::template word2<8>(spat, rho, acc);
+          else
+            Pat<P0, 0, NS>::template word2<1>(spat, rho, acc);
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          const u64 w = w0 + (u64)(wi + k) * stride;
-          const u64 s = ~(acc[k * 2] | acc[k * 2 + 1]);
-          if (w != 0 && w < wfull && wi + k < it.Tc) {
-            sv[k] = s;  // an interior word: every period is in range
+          for (int k = 0; k < 2; ++k) {
+            const u64 w = w0 + (u64)(wi + k) * stride;
+            const u64 s = ~(acc[k * 2] | acc[k * 2 + 1]);
+            if (w != 0 && w < wfull && wi + k < it.Tc) {
+              sv[k] = s;  // an interior word: every period is in range
+              continue;
+            }
+            if (wi + k >= it.Tc || 64ull * w >= U) continue;
+            const u64 left = U - 64ull * w;
+            u64 valid = left >= 64 ? ~0ull : ((1ull << left) - 1ull);
+            if (w == 0 && R < it.lo_off) valid &= ~1ull;
+            if (left <= 64 && R >= it.hi_last) valid &= ~(1ull << (left - 1));
+            sv[k] = s & valid;
+          }
+        }
+        // push the survivors into the warp's queue; drain first when they
+        // do not fit, and when one step alone overfills an empty queue
+        // push the prefix that fits and drain again (every pass pushes or
+        // drains, so it ends)
+        for (;;) {
+          const u32 c = __popcll(sv[0]) + __popcll(sv[1]);
+          const u32 tot = __reduce_add_sync(0xffffffffu, c);
+          if (tot == 0) break;
+          if (qn + tot > kWq && qn > 0) {
+            drain_any(wq, wq2, qn, S, e, it, gitem, a, wq_short, ntest);
+            qn = 0;
             continue;
           }
-          if (wi + k >= it.Tc || 64ull * w >= U) continue;
-          const u64 left = U - 64ull * w;
-          u64 valid = left >= 64 ? ~0ull : ((1ull << left) - 1ull);
-          if (w == 0 && R < it.lo_off) valid &= ~1ull;
-          if (left <= 64 && R >= it.hi_last) valid &= ~(1ull << (left - 1));
-          sv[k] = s & valid;
-        }
-      }
-      // push the survivors into the warp's queue; drain first when they
-      // do not fit, and when one step alone overfills an empty queue push
-      // the prefix that fits and drain again (every pass pushes or drains,
-      // so it ends)
-      for (;;) {
-        const u32 c = __popcll(sv[0]) + __popcll(sv[1]);
-        const u32 tot = __reduce_add_sync(0xffffffffu, c);
-        if (tot == 0) break;
-        if (qn + tot > kWq && qn > 0) {
-          drain_any(wq, wq2, qn, S, e, it, gitem, a, wq_short, ntest);
-          qn = 0;
-          continue;
-        }
-        // exclusive prefix of c over the warp
-        u32 x = c;
+          // exclusive prefix of c over the warp
+          u32 x = c;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const u32 y = __shfl_up_sync(0xffffffffu, x, o);
-          if (wl >= (u32)o) x += y;
-        }
-        u32 pos = qn + x - c;
-        const u32 end = min(qn + tot, (u32)kWq);
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          while (sv[k] && pos < end) {
-            const int b = __ffsll((long long)sv[k]) - 1;
-            sv[k] &= sv[k] - 1;
-            wq[pos++] = ((u32)tid << 22) | ((wi + k) << 6) | (u32)b;
+          for (int o = 1; o < 32; o <<= 1) {
+            const u32 y = __shfl_up_sync(0xffffffffu, x, o);
+            if (wl >= (u32)o) x += y;
           }
+          u32 pos = qn + x - c;
+          const u32 end = min(qn + tot, (u32)kWq);
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            while (sv[k] && pos < end) {
+              const int b = __ffsll((long long)sv[k]) - 1;
+              sv[k] &= sv[k] - 1;
+              wq[pos++] = ((u32)tid << 22) | ((wi + k) << 6) | (u32)b;
+            }
+          }
+          __syncwarp();
+          if (qn + tot <= (u32)kWq) {
+            qn += tot;
+            break;
+          }
+          drain_any(wq, wq2, kWq, S, e, it, gitem, a, wq_short, ntest);
+          qn = 0;
         }
-        __syncwarp();
-        if (qn + tot <= (u32)kWq) {
-          qn += tot;
-          break;
-        }
-        drain_any(wq, wq2, kWq, S, e, it, gitem, a, wq_short, ntest);
-        qn = 0;
       }
+      // every queued code refers to this warp task's chains: drain them
+      // before the warp's threads take the next task's chains
+      drain_any(wq, wq2, qn, S, e, it, gitem, a, wq_short, ntest);
     }
-    drain_any(wq, wq2, qn, S, e, it, gitem, a, wq_short, ntest);
+    u64 nt = ntest, nw = nword;  // warp sums in 64 bits
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      ntest += __shfl_down_sync(0xffffffffu, ntest, o);
-      nword += __shfl_down_sync(0xffffffffu, nword, o);
+      nt += __shfl_down_sync(0xffffffffu, nt, o);
+      nw += __shfl_down_sync(0xffffffffu, nw, o);
     }
     if (wl == 0) {
-      if (ntest) atomicAdd(&a.ctr->s2_tests, (unsigned long long)ntest);
-      if (nword) atomicAdd(&a.ctr->s1_words, (unsigned long long)nword);
+      if (nt) atomicAdd(&a.ctr->s2_tests, (unsigned long long)nt);
+      if (nw) atomicAdd(&a.ctr->s1_words, (unsigned long long)nw);
     }
     __syncthreads();
   }

@@ -74,7 +74,7 @@ class Tuning(ctypes.Structure):
                 ("capacity_scale", ctypes.c_float),
                 ("round_cut", ctypes.c_float), ("group_lane_words", _u32),
                 ("mark_segment", _u32), ("pattern_primes", _u32),
-                ("mark_pattern_primes", _u32)]
+                ("mark_pattern_primes", _u32), ("warp_tasks", _u32)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -7,7 +7,8 @@ batches overlap on the device while the host collects one and fills the
 other.
 
 Requests are cut into chunks of at most ``chunk`` units of their engine's
-line variable (p, or j = k / W for Dickson) and queued chunk by chunk in
+line variable (p, or j = k / W for Dickson), and of at most a quarter of
+the HBM budget's predicted footprint, and queued chunk by chunk in
 arrival order.  Whenever a slot is free it takes queued chunks, oldest
 first, while the batch stays under a work budget (``batch_work`` line
 units) and an HBM budget, and submits them as one persistent launch; a
@@ -69,15 +70,27 @@ class ServeLoop:
         expect = (hi - lo) * e.survival + 64
         return 4 * e.NP + int(2 * expect) * ENTRY_BYTES + 256
 
+    def chunk_units(self, iv):
+        """Line units per chunk of this request: at most `chunk`, and at
+        most what keeps one chunk's predicted footprint within a quarter of
+        the HBM budget, so no single chunk -- always admitted, even alone
+        over the budget -- grows a slot's buffers past what batches of the
+        budget need (a growth reallocates gigabytes while requests wait)."""
+        e = self._engine(iv)
+        per_unit = 2 * e.survival * ENTRY_BYTES
+        cap = int(self.hbm_budget / 4 / per_unit) if per_unit > 0 else self.chunk
+        return min(self.chunk, max(1 << 20, cap))
+
     def chunks(self, iv):
-        """The request as intervals of at most `chunk` line units, in
-        order; each is an Interval of the same engine and threshold."""
+        """The request as intervals of at most `chunk_units` line units,
+        in order; each is an Interval of the same engine and threshold."""
         W = self._engine(iv).W if iv.kind == DICKSON else 1
         lo, hi = line_range(iv, W)
+        step = self.chunk_units(iv)
         out = []
         a = lo
         while a < hi:
-            b = min(hi, a + self.chunk)
+            b = min(hi, a + step)
             if iv.kind == DICKSON:   # back to k: [a*W, b*W) covers j in [a, b)
                 klo = iv.lo if a == lo else a * W
                 khi = iv.hi if b == hi else b * W
@@ -93,8 +106,13 @@ class ServeLoop:
         """requests: [(arrival_s, Interval)] sorted by arrival.  Returns
         (per request (offsets, depths) as the batch engine gives them for
         the whole request, latency_s per request, stats)."""
+        # tables resident up front: every engine a chunk will run on (the
+        # wheel follows an interval's length, so a chunk can run on another
+        # engine than its whole request), so none is built while requests
+        # wait
         for _, iv in requests:
-            self._engine(iv)                    # tables resident up front
+            for c in self.chunks(iv):
+                self._engine(c)
         for s in self.slots:
             s._ensure()
         gc.collect()

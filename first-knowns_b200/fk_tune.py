@@ -13,7 +13,8 @@ compaction round is cut (``round_cut``: lower means fewer, longer rounds),
 and three kernel-variant choices: the marking segment length in bytes
 (``mark_segment``: 16, 32 or 64 KiB of shared byte map) and the pattern
 primes each CTA stages in shared memory, per sieve kernel
-(``pattern_primes``, ``mark_pattern_primes``: 24, 32 or 40).
+(``pattern_primes``, ``mark_pattern_primes``: 24, 32 or 40), and the
+blocks of chains per CTA task of the rounds kernel (``warp_tasks``).
 None of them can change a result; they only move time.
 
 ``tune`` runs coordinate descent: starting from the current setting it
@@ -44,6 +45,7 @@ SPACE = {
     "pattern_primes": [24, 40],
     "mark_pattern_primes": [24, 40],
     "mark_segment": [16384, 65536],
+    "warp_tasks": [16, 32],
 }
 
 DEFAULT_PATH = pathlib.Path(__file__).resolve().parent / "tuning.json"

@@ -192,6 +192,11 @@ typedef struct fk_tuning {
                                   * candidate                                 */
   uint32_t mark_pattern_primes;  /* the same for the marking sieve (24, 32 or *
                                   * 40); the primes past them are marked      */
+  uint32_t warp_tasks;           /* pattern sieve + rounds: blocks of 32      *
+                                  * threads' chains per CTA task (8, 16 or    *
+                                  * 32), claimed by the CTA's warps one at a  *
+                                  * time; the CTA waits for its slowest warp  *
+                                  * once per task                             */
 } fk_tuning;
 fk_status fk_batch_set_tuning(fk_batch* b, const fk_tuning* t);
 fk_status fk_batch_get_tuning(const fk_batch* b, fk_tuning* out);

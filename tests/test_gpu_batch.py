@@ -166,13 +166,15 @@ def test_tuning_changes_no_result():
                      mark_segment=65536, mark_bias=0.25),
                 dict(pattern_primes=32, mark_pattern_primes=32,
                      mark_segment=65536, seg_per_task=1, mark_bias=2.0),
+                dict(warp_tasks=16, warp_lane_words=32),
+                dict(warp_tasks=32, group_lane_words=8, chains_per_sm=8192),
                 dict(sieve_ctas_per_sm=3, mark_ctas_per_sm=3,
                      classify_ctas_per_sm=8, mark_limit=65536,
                      seg_per_task=8, warp_queue=32, mark_bias=1.0,
                      chains_per_sm=2048, warp_lane_words=256,
                      round_cut=0.5, group_lane_words=32,
                      pattern_primes=32, mark_pattern_primes=32,
-                     mark_segment=32768)]
+                     mark_segment=32768, warp_tasks=8)]
     for kw in settings:
         be.set_tuning(**kw)
         assert _same(be.run_arrays(ivs, graph=True), ref), kw
@@ -189,6 +191,8 @@ def test_tuning_changes_no_result():
         be.set_tuning(pattern_primes=33)
     with pytest.raises(ValueError):
         be.set_tuning(mark_pattern_primes=16)
+    with pytest.raises(ValueError):
+        be.set_tuning(warp_tasks=12)
 
 
 def test_overflow_grows_the_buffers_and_reruns():

@@ -148,3 +148,25 @@ def test_long_intervals_take_the_wider_wheel(monkeypatch):
     assert es.key_for(dk)[-1] == fk_batch.P0_WIDE
     narrow = fk_batch.EngineSet(wide=False)
     assert narrow.key_for(long_)[-1] == fk_batch.P0_NARROW
+
+
+def test_serving_chunks_keep_their_footprint_within_the_budget():
+    """A chunk's predicted footprint (twice the survival estimate's
+    survivors, ENTRY_BYTES each) stays within a quarter of the HBM budget;
+    the line-unit cap still applies, and the chunks tile the request."""
+    import types
+    import fk_serve
+    import fk_workloads as W
+    loop = fk_serve.ServeLoop.__new__(fk_serve.ServeLoop)
+    loop.chunk, loop.hbm_budget = 1 << 30, 1 << 30
+    eng = types.SimpleNamespace(survival=1e-2, W=1, NP=6542, M=30030)
+    loop._engine = lambda iv: eng
+    iv = W.Interval(W.EULER, 6, 10 ** 12, 10 ** 12 + (1 << 34), 6, 64)
+    units = loop.chunk_units(iv)
+    assert 2 * eng.survival * units * fk_serve.ENTRY_BYTES <= loop.hbm_budget / 4
+    cs = loop.chunks(iv)
+    assert cs[0].lo == iv.lo and cs[-1].hi == iv.hi
+    assert all(a.hi == b.lo for a, b in zip(cs, cs[1:]))
+    assert all(c.hi - c.lo <= units for c in cs)
+    eng.survival = 1e-9                         # the line-unit cap binds
+    assert loop.chunk_units(iv) == loop.chunk
