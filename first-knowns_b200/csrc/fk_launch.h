@@ -1,9 +1,10 @@
 // fk_launch.h -- launchers of the sieve kernels' template variants.
 //
-// k_sieve<P0, NS> and k_mark<P0, NS, SEG> come in one variant per wheel
-// family P0 (6, 7, 9, 11), pattern-prime count NS (24, 32, 40) and, for
-// the marking sieve, segment length SEG (16384, 32768, 65536 periods): 12
-// and 36 kernels.  They are instantiated in their own translation units
+// k_sieve<P0, NS, DYN> and k_mark<P0, NS, SEG> come in one variant per
+// wheel family P0 (6, 7, 9, 11), pattern-prime count NS (24, 32, 40), for
+// the rounds kernel with or without warps claiming blocks of chains (DYN),
+// and for the marking sieve per segment length SEG (16384, 32768, 65536
+// periods): 24 and 36 kernels.  They are instantiated in their own translation units
 // (fk_sieve_k.cu, fk_mark_k6.cu ... fk_mark_k11.cu), which the build
 // compiles in parallel, and reached through the plain functions below.
 #pragma once

@@ -436,9 +436,117 @@ __device__ __forceinline__ bool stage_patterns(u64* spat, const DevEngine& eg,
   return *status == 0;
 }
 
-// NS: the pattern primes this variant stages (the engine descriptor's NS
-// and round cuts must match it).
+// One block of 32 threads' chains (a warp task): thread wl of the warp
+// sweeps chain gw + (wl >> gsh) of the item, pushes its pattern survivors
+// into the warp's queue and drains it through the compaction rounds; the
+// queue is empty again on return.
 template <int P0, int NS>
+__device__ __forceinline__ void sieve_block(
+    const u64* __restrict__ spat, SieveSmem& S, const SieveArgs& a,
+    const DevEngine& e, const DevItem& it, u32 gitem, u64 gw, u64 nchain,
+    u32 G, u32 gsh, u32 wq_short, u64 wfull, u32& ntest, u32& nword) {
+  const int tid = threadIdx.x;
+  const u32 wl = tid & 31, wid = tid >> 5;
+  const u64 U = it.U;
+  const u32 stride = G;
+  u32* wq = S.qa + wid * kWq;
+  u32* wq2 = S.qb + wid * kWq;
+  // ---- this thread's chain -----------------------------------------
+  const u64 g = gw + (wl >> gsh);
+  const bool active = g < nchain;
+  const u64 chunk = active ? g / e.L : 0;
+  const u32 lane = active ? (u32)(g % e.L) : 0;
+  const u64 R = active ? e.lanes[lane] : 0;
+  const u64 w0 = chunk * (u64)G * it.Tc + (wl & (G - 1));
+  S.chain_R[tid] = R;
+  S.chain_w0[tid] = w0;
+  u32 rho[NS];
+  Pat<P0, 0, NS>::setup(rho, R, 64ull * w0, a.xq + it.xq_off, S.minv);
+  u32 qn = 0;
+  if (active) {
+    // the chain's words in range: j < Tc with w0 + j*stride < ceil(U/64)
+    const u64 wend = (U + 63) >> 6;
+    if (w0 < wend)
+      nword += (u32)min((u64)it.Tc, (wend - w0 + stride - 1) / stride);
+  }
+  __syncwarp();
+  for (u32 wi = 0; wi < it.Tc; wi += 2) {
+    // two words of the chain: j = wi and wi + 1
+    u64 sv[2] = {0, 0};
+    if (active) {
+      u64 acc[4] = {0, 0, 0, 0};
+      if (G == 32)
+        Pat<P0, 0, NS>::template word2<32>(spat, rho, acc);
+      else if (G == 8)
+        Pat<P0, 0, NS>::template word2<8>(spat, rho, acc);
+      else
+        Pat<P0, 0, NS>::template word2<1>(spat, rho, acc);
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const u64 w = w0 + (u64)(wi + k) * stride;
+        const u64 s = ~(acc[k * 2] | acc[k * 2 + 1]);
+        if (w != 0 && w < wfull && wi + k < it.Tc) {
+          sv[k] = s;  // an interior word: every period is in range
+          continue;
+        }
+        if (wi + k >= it.Tc || 64ull * w >= U) continue;
+        const u64 left = U - 64ull * w;
+        u64 valid = left >= 64 ? ~0ull : ((1ull << left) - 1ull);
+        if (w == 0 && R < it.lo_off) valid &= ~1ull;
+        if (left <= 64 && R >= it.hi_last) valid &= ~(1ull << (left - 1));
+        sv[k] = s & valid;
+      }
+    }
+    // push the survivors into the warp's queue; drain first when they
+    // do not fit, and when one step alone overfills an empty queue
+    // push the prefix that fits and drain again (every pass pushes or
+    // drains, so it ends)
+    for (;;) {
+      const u32 c = __popcll(sv[0]) + __popcll(sv[1]);
+      const u32 tot = __reduce_add_sync(0xffffffffu, c);
+      if (tot == 0) break;
+      if (qn + tot > kWq && qn > 0) {
+        drain_any(wq, wq2, qn, S, e, it, gitem, a, wq_short, ntest);
+        qn = 0;
+        continue;
+      }
+      // exclusive prefix of c over the warp
+      u32 x = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const u32 y = __shfl_up_sync(0xffffffffu, x, o);
+        if (wl >= (u32)o) x += y;
+      }
+      u32 pos = qn + x - c;
+      const u32 end = min(qn + tot, (u32)kWq);
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        while (sv[k] && pos < end) {
+          const int b = __ffsll((long long)sv[k]) - 1;
+          sv[k] &= sv[k] - 1;
+          wq[pos++] = ((u32)tid << 22) | ((wi + k) << 6) | (u32)b;
+        }
+      }
+      __syncwarp();
+      if (qn + tot <= (u32)kWq) {
+        qn += tot;
+        break;
+      }
+      drain_any(wq, wq2, kWq, S, e, it, gitem, a, wq_short, ntest);
+      qn = 0;
+    }
+  }
+  // every queued code refers to this warp task's chains: drain them
+  // before the warp's threads take the next task's chains
+  drain_any(wq, wq2, qn, S, e, it, gitem, a, wq_short, ntest);
+}
+
+// NS: the pattern primes this variant stages (the engine descriptor's NS
+// and round cuts must match it).  DYN: the CTA's warps claim blocks of
+// chains from a shared counter (a.warp_tasks blocks per task); without it
+// each warp takes exactly its own block (a.warp_tasks = 8), which holds
+// fewer registers across the word loop.
+template <int P0, int NS, bool DYN>
 __global__ void __launch_bounds__(kBlock, 3) k_sieve(SieveArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   u64* spat = reinterpret_cast<u64*>(smem_raw);
@@ -504,110 +612,27 @@ __global__ void __launch_bounds__(kBlock, 3) k_sieve(SieveArgs a) {
     const u64 nchain = it.nchunk * e.L;
     const u64 wt0 = (task - a.task_prefix[S.item]) * (u64)a.warp_tasks;
     const u32 cpw = 32u >> gsh;  // chains per warp task
-    const u64 U = it.U;
-    u32* wq = S.qa + wid * kWq;
-    u32* wq2 = S.qb + wid * kWq;
     const u32 wq_short = a.warp_queue;
-    const u32 stride = G;
     // words below wfull end before the item's last period, so only the
     // first word (lo_off) and the last (hi_last, U) need a validity mask
-    const u64 wfull = U ? (U - 1) >> 6 : 0;
+    const u64 wfull = it.U ? (it.U - 1) >> 6 : 0;
     u32 ntest = 0, nword = 0;  // this CTA task's counts
-    for (;;) {
-      u32 wt = 0;
-      if (wl == 0) wt = atomicAdd(&S.wnext, 1u);
-      wt = __shfl_sync(0xffffffffu, wt, 0);
-      if (wt >= a.warp_tasks) break;
-      const u64 gw = (wt0 + wt) * cpw;       // the warp task's first chain
-      if (gw >= nchain) break;               // and every later one's too
-      // ---- this thread's chain -----------------------------------------
-      const u64 g = gw + (wl >> gsh);
-      const bool active = g < nchain;
-      const u64 chunk = active ? g / e.L : 0;
-      const u32 lane = active ? (u32)(g % e.L) : 0;
-      const u64 R = active ? e.lanes[lane] : 0;
-      const u64 w0 = chunk * (u64)G * it.Tc + (wl & (G - 1));
-      S.chain_R[tid] = R;
-      S.chain_w0[tid] = w0;
-      u32 rho[NS];
-      Pat<P0, 0, NS>::setup(rho, R, 64ull * w0, a.xq + it.xq_off, S.minv);
-      u32 qn = 0;
-      if (active) {
-        // the chain's words in range: j < Tc with w0 + j*stride < ceil(U/64)
-        const u64 wend = (U + 63) >> 6;
-        if (w0 < wend)
-          nword += (u32)min((u64)it.Tc, (wend - w0 + stride - 1) / stride);
+    if (DYN) {
+      for (;;) {
+        u32 wt = 0;
+        if (wl == 0) wt = atomicAdd(&S.wnext, 1u);
+        wt = __shfl_sync(0xffffffffu, wt, 0);
+        if (wt >= a.warp_tasks) break;
+        const u64 gw = (wt0 + wt) * cpw;     // the warp task's first chain
+        if (gw >= nchain) break;             // and every later one's too
+        sieve_block<P0, NS>(spat, S, a, e, it, gitem, gw, nchain, G, gsh,
+                            wq_short, wfull, ntest, nword);
       }
-      __syncwarp();
-      for (u32 wi = 0; wi < it.Tc; wi += 2) {
-        // two words of the chain: j = wi and wi + 1
-        u64 sv[2] = {0, 0};
-        if (active) {
-          u64 acc[4] = {0, 0, 0, 0};
-          if (G == 32)
-            Pat<P0, 0, NS>::template word2<32>(spat, rho, acc);
-          else if (G == 8)
-            Pat<P0, 0, NS>::template word2<8>(spat, rho, acc);
-          else
-            Pat<P0, 0, NS>::template word2<1>(spat, rho, acc);
-#pragma unroll
-          for (int k = 0; k < 2; ++k) {
-            const u64 w = w0 + (u64)(wi + k) * stride;
-            const u64 s = ~(acc[k * 2] | acc[k * 2 + 1]);
-            if (w != 0 && w < wfull && wi + k < it.Tc) {
-              sv[k] = s;  // an interior word: every period is in range
-              continue;
-            }
-            if (wi + k >= it.Tc || 64ull * w >= U) continue;
-            const u64 left = U - 64ull * w;
-            u64 valid = left >= 64 ? ~0ull : ((1ull << left) - 1ull);
-            if (w == 0 && R < it.lo_off) valid &= ~1ull;
-            if (left <= 64 && R >= it.hi_last) valid &= ~(1ull << (left - 1));
-            sv[k] = s & valid;
-          }
-        }
-        // push the survivors into the warp's queue; drain first when they
-        // do not fit, and when one step alone overfills an empty queue
-        // push the prefix that fits and drain again (every pass pushes or
-        // drains, so it ends)
-        for (;;) {
-          const u32 c = __popcll(sv[0]) + __popcll(sv[1]);
-          const u32 tot = __reduce_add_sync(0xffffffffu, c);
-          if (tot == 0) break;
-          if (qn + tot > kWq && qn > 0) {
-            drain_any(wq, wq2, qn, S, e, it, gitem, a, wq_short, ntest);
-            qn = 0;
-            continue;
-          }
-          // exclusive prefix of c over the warp
-          u32 x = c;
-#pragma unroll
-          for (int o = 1; o < 32; o <<= 1) {
-            const u32 y = __shfl_up_sync(0xffffffffu, x, o);
-            if (wl >= (u32)o) x += y;
-          }
-          u32 pos = qn + x - c;
-          const u32 end = min(qn + tot, (u32)kWq);
-#pragma unroll
-          for (int k = 0; k < 2; ++k) {
-            while (sv[k] && pos < end) {
-              const int b = __ffsll((long long)sv[k]) - 1;
-              sv[k] &= sv[k] - 1;
-              wq[pos++] = ((u32)tid << 22) | ((wi + k) << 6) | (u32)b;
-            }
-          }
-          __syncwarp();
-          if (qn + tot <= (u32)kWq) {
-            qn += tot;
-            break;
-          }
-          drain_any(wq, wq2, kWq, S, e, it, gitem, a, wq_short, ntest);
-          qn = 0;
-        }
-      }
-      // every queued code refers to this warp task's chains: drain them
-      // before the warp's threads take the next task's chains
-      drain_any(wq, wq2, qn, S, e, it, gitem, a, wq_short, ntest);
+    } else {
+      // this warp's own block (a block past the item's chains runs with
+      // every thread inactive and emits nothing)
+      sieve_block<P0, NS>(spat, S, a, e, it, gitem, (wt0 + wid) * cpw,
+                          nchain, G, gsh, wq_short, wfull, ntest, nword);
     }
     u64 nt = ntest, nw = nword;  // warp sums in 64 bits
 #pragma unroll

@@ -12,14 +12,23 @@ size_t sieve_smem() {
 
 template <int P0, int NS>
 cudaError_t sieve_limit() {
-  return cudaFuncSetAttribute(k_sieve<P0, NS>,
+  cudaError_t r = cudaFuncSetAttribute(
+      k_sieve<P0, NS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      (int)sieve_smem<P0, NS>());
+  if (r != cudaSuccess) return r;
+  return cudaFuncSetAttribute(k_sieve<P0, NS, true>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)sieve_smem<P0, NS>());
 }
 
+// Eight blocks per task is one per warp: the variant without the shared
+// counter; more blocks per task take the claiming variant.
 template <int P0, int NS>
 cudaError_t sieve_launch(u32 grid, cudaStream_t s, const SieveArgs& a) {
-  k_sieve<P0, NS><<<grid, kBlock, sieve_smem<P0, NS>(), s>>>(a);
+  if (a.warp_tasks == kBlock / 32)
+    k_sieve<P0, NS, false><<<grid, kBlock, sieve_smem<P0, NS>(), s>>>(a);
+  else
+    k_sieve<P0, NS, true><<<grid, kBlock, sieve_smem<P0, NS>(), s>>>(a);
   return cudaGetLastError();
 }
 

@@ -115,12 +115,38 @@ class ServeLoop:
                 self._engine(c)
         for s in self.slots:
             s._ensure()
+        self._prime(requests)
         gc.collect()
         gc.freeze()
         try:
             return self._run(requests, time_limit)
         finally:
             gc.unfreeze()
+
+    def _prime(self, requests):
+        """Run, on every slot and before the clock starts, one batch of
+        the requests' largest-footprint chunks that fits the budgets, so
+        the slots' device and pinned buffers already have the size a batch
+        can need (a slot whose engine set grew starts with none, and
+        growing them under load reallocates while requests wait)."""
+        cs = [(self.footprint(c), i, c) for i, c in enumerate(
+            c for _, iv in requests for c in self.chunks(iv))]
+        cs.sort(key=lambda x: (-x[0], x[1]))
+        take, foot, work = [], 0, 0
+        for f, _, c in cs:
+            e = self._engine(c)
+            lo, hi = line_range(c, e.W if c.kind == DICKSON else 1)
+            if take and (foot + f > self.hbm_budget or
+                         work + (hi - lo) > self.batch_work or
+                         len(take) >= self.max_items):
+                continue
+            take.append(c)
+            foot += f
+            work += hi - lo
+        if take:
+            for s in self.slots:
+                s.submit(take)
+                s.wait_arrays()
 
     def _run(self, requests, time_limit):
         n = len(requests)
