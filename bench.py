@@ -587,10 +587,17 @@ def bench_fk(args):
         tb = BatchEngine(sample, engset=eng.engset)
         res = fk_tune.tune(tb, sample, budget_s=args.tune_seconds)
         eng.set_tuning(**res["best"])
+        start = res["trials"][0]["setting"]
         tuning = {"source": "fk_tune coordinate descent on a 1/16 sample "
                             "(seed + 1000)",
                   "setting": res["best"], "trials": len(res["trials"]),
-                  "seconds": round(res["seconds"], 1)}
+                  "seconds": round(res["seconds"], 1),
+                  # each trial: the fields it changed from the starting
+                  # setting, and its device ms on the sample
+                  "trial_log": [
+                      [{k: v for k, v in t["setting"].items()
+                        if start.get(k) != v}, round(t["ms"], 1)]
+                      for t in res["trials"]]}
         del tb
     else:
         tuning = {"source": "defaults", "setting": eng.tuning()}

@@ -1327,6 +1327,28 @@ void fk_batch_destroy(fk_batch* b) {
   delete b;
 }
 
+fk_status fk_batch_add_engines(fk_batch* b, fk_engine* const* engines,
+                               uint32_t nengines) {
+  if (!b || (!engines && nengines)) return set_err(FK_ERR_ARG, "null argument");
+  if (b->pending) return set_err(FK_ERR_ARG, "a submitted run is pending");
+  if (nengines == 0) return FK_OK;
+  for (uint32_t i = 0; i < nengines; ++i)
+    if (!engines[i]) return set_err(FK_ERR_ARG, "null engine");
+  // the descriptor array grows; every other buffer keeps its size and
+  // contents, and the captured graph (which holds the old array's address)
+  // is dropped
+  const size_t n = b->engines.size() + nengines;
+  DevEngine* nd = nullptr;
+  FK_CUDA(cudaMalloc(&nd, sizeof(DevEngine) * n));
+  cudaFree(b->d_engines);
+  b->d_engines = nd;
+  b->engines.insert(b->engines.end(), engines, engines + nengines);
+  if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+  if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+  b->graph_key.clear();
+  return apply_tuning(b);
+}
+
 static void fill_result(fk_batch* b, fk_batch_result* out) {
   out->nitems = b->user.size();
   out->item_start = b->r_start.data();

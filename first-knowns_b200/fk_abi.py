@@ -114,6 +114,9 @@ SIGNATURES = {
                                          _u32,
                                          ctypes.POINTER(ctypes.c_void_p)]),
     "fk_batch_destroy": (None, [ctypes.c_void_p]),
+    "fk_batch_add_engines": (ctypes.c_int32, [ctypes.c_void_p,
+                                              ctypes.POINTER(ctypes.c_void_p),
+                                              ctypes.c_uint32]),
     "fk_batch_run": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(Item),
                                       _u64, ctypes.c_int,
                                       ctypes.POINTER(BatchResult)]),
@@ -304,6 +307,16 @@ class Batch:
         h = ctypes.c_void_p()
         _check(lib.fk_batch_create(arr, len(self._engines), ctypes.byref(h)))
         self._h, self._lib = h, lib
+
+    def add_engines(self, engines):
+        """Append engines (indexed after the existing ones); the batch's
+        buffers are kept."""
+        new = list(engines)
+        if not new:
+            return
+        arr = (ctypes.c_void_p * len(new))(*[e.handle for e in new])
+        _check(self._lib.fk_batch_add_engines(self._h, arr, len(new)))
+        self._engines.extend(new)
 
     def close(self):
         if getattr(self, "_h", None):

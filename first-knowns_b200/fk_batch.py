@@ -95,14 +95,17 @@ class BatchEngine:
         self._nengines = -1
 
     def _ensure(self):
-        n = len(self.engset.engines())
-        if self._batch is None or n != self._nengines:
-            if self._batch is not None:
-                self._batch.close()
-            self._batch = fk_abi.Batch(self.engset.engines())
-            self._nengines = n
+        engines = self.engset.engines()
+        if self._batch is None:
+            self._batch = fk_abi.Batch(engines)
+            self._nengines = len(engines)
             if getattr(self, "_tuning", None):
                 self._batch.set_tuning(**self._tuning)
+        elif len(engines) != self._nengines:
+            # engines are only ever appended to the set: extend the batch
+            # in place, keeping its buffers
+            self._batch.add_engines(engines[self._nengines:])
+            self._nengines = len(engines)
         return self._batch
 
     def run_arrays(self, intervals, graph=True):

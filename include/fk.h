@@ -138,6 +138,12 @@ fk_status fk_depths(fk_engine* e, const uint64_t* x_limbs, uint64_t count,
 fk_status fk_batch_create(fk_engine* const* engines, uint32_t nengines,
                           fk_batch** out);
 void fk_batch_destroy(fk_batch* b);
+/* Appends engines to a batch (item.engine indexes them after the existing
+ * ones).  The batch keeps its device and pinned buffers, so a caller that
+ * meets new engine configurations while it serves does not rebuild (and
+ * regrow) them.  No counterpart in the reference: batching is new here. */
+fk_status fk_batch_add_engines(fk_batch* b, fk_engine* const* engines,
+                               uint32_t nengines);
 /* Runs all items; use_graph != 0 replays a captured CUDA graph. */
 fk_status fk_batch_run(fk_batch* b, const fk_item* items, uint64_t nitems,
                        int use_graph, fk_batch_result* out);

@@ -248,3 +248,20 @@ def test_wide_wheel_intervals_match_the_narrow_wheel():
     a = wide.run_arrays(ivs)
     assert _same(a, narrow.run_arrays(ivs))
     assert sum(x[0].size for x in a[:3]) > 100
+
+
+def test_engines_added_to_a_batch_keep_its_results():
+    """A batch that meets new engines is extended in place
+    (fk_batch_add_engines): its later runs, graph and eager, over the old
+    and the new engines equal those of a batch built with all of them."""
+    from fk_batch import BatchEngine
+    ivs = _clipped(60, 91)
+    be = BatchEngine(ivs[:3])
+    n0 = len(be.engset.engines())
+    be.run_arrays(ivs[:3], graph=True)         # buffers and a graph
+    b0 = be._batch
+    got_g = be.run_arrays(ivs, graph=True)     # new engines: extended
+    assert len(be.engset.engines()) > n0 and be._batch is b0
+    got_e = be.run_arrays(ivs, graph=False)
+    want = BatchEngine(ivs).run_arrays(ivs, graph=False)
+    assert _same(got_g, want) and _same(got_e, want)
