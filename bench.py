@@ -93,6 +93,9 @@ def parse():
                     help="run one profiling case (PROFILE_CASES) and exit")
     ap.add_argument("--runs", type=int, default=2,
                     help="--profile-case: runs (the first is a warm-up)")
+    ap.add_argument("--peaks", action="store_true",
+                    help="print every fk_peak probe (the rooflines' "
+                         "measured denominators) three times and exit")
     ap.add_argument("--set", action="append", default=[],
                     metavar="FIELD=VALUE",
                     help="--profile-case: an fk_tuning field to set "
@@ -701,9 +704,10 @@ def bench_fk(args):
             "residue) hit",
             "measured on this GPU by fk_peak (conflict-free st.shared.u8, "
             "32 lanes)",
-            "DRAM bytes do not grow with the work (tables stay in L2 and "
-            "shared memory): ncu of the AP n = 6 case reads 0.7 MB per "
-            "launch (profiles/), so a scaled figure would be meaningless"),
+            "DRAM bytes do not grow with the marks (tables stay in L2 and "
+            "shared memory): ncu of the long mixed case reads 9.1 MB and "
+            "writes 95 MB (the candidate list) per launch (profiles/), so "
+            "a figure scaled by marks would be meaningless"),
         "k_sieve": roof(
             "k_sieve (pattern sieve + compaction rounds)", "imad",
             9 * st["s2_tests"], rnd_s, imad_peak, "G int-multiply-adds/s",
@@ -714,8 +718,9 @@ def bench_fk(args):
             "measured on this GPU by fk_peak (32-bit mad.lo/mad.hi "
             "chains, 8 per thread)",
             "DRAM traffic is the lane table read once (8 B per lane) plus "
-            "the candidates written; ncu of the Euler n = 17 window: "
-            "246 MB read for a 240 MB table (profiles/)"),
+            "the candidates written; ncu of the long mixed case: 6.7 MB "
+            "read per launch, of the Euler n = 17 window: 246 MB read for "
+            "a 240 MB lane table (profiles/)"),
     }
     times = {"k_classify": cls_s, "k_mark": mark_s, "k_sieve": rnd_s}
     dominant = roofs[max(times, key=times.get)]
@@ -797,6 +802,13 @@ def main():
     if args.profile_case:
         return run_profile_case(args.profile_case, args.runs,
                                 tuning_overrides(args.set))
+    if args.peaks:
+        import fk_abi
+        for name in fk_abi.PEAKS:
+            vals = [fk_abi.peak(name) for _ in range(3)]
+            print(f"{name}: " + ", ".join(f"{v:.4g}" for v in vals),
+                  flush=True)
+        return 0
     if args.impl == "reference":
         return bench_reference(args)
     return bench_fk(args)
