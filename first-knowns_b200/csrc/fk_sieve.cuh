@@ -156,6 +156,19 @@ struct Pat {
     k[I] = (u32)(((u32)(u0 % q) * i64 + s) % q);
     Pat<P0, I + 1, NS>::setup(k, R, u0, xq, s_minv);
   }
+  // The table indexes of a warp sweeping one lane, thread wl from word
+  // base + wl: (base_I + wl) mod q, base_I held by thread I (b0) or, for
+  // I >= 32, by thread I - 32 (b1).
+  static __device__ __forceinline__ void spread(u32* k, u32 b0, u32 b1,
+                                                u32 wl) {
+    constexpr u32 q = fk_nth_prime(P0 + I);
+    const u32 b = __shfl_sync(0xffffffffu, I < 32 ? b0 : b1, I & 31);
+    // wl < 32: below q from the 37 up; the 17 ... 31 of the 13# and 17#
+    // families reduce it first, so one subtraction still ends in [0, q)
+    const u32 r = b + (q > 31 ? wl : wl % q);
+    k[I] = min(r, r - q);
+    Pat<P0, I + 1, NS>::spread(k, b0, b1, wl);
+  }
 };
 template <int P0, int NS>
 struct Pat<P0, NS, NS> {
@@ -163,7 +176,23 @@ struct Pat<P0, NS, NS> {
   static __device__ __forceinline__ void word2(const u64*, u32*, u64*) {}
   static __device__ __forceinline__ void setup(u32*, u64, u64, const u32*,
                                                const u32*) {}
+  static __device__ __forceinline__ void spread(u32*, u32, u32, u32) {}
 };
+
+// Pattern prime I's table index at word wb of lane R: (wb + s) mod q with
+// s = (X0 + R) * (M mod q)^-1 * 64^-1 mod q the lane's phase (xq holds X0
+// mod q, s_minv the product of the two inverses), from the prime's record.
+__device__ __forceinline__ u32 lane_base(const DevEngine& e,
+                                         const u32* __restrict__ xq,
+                                         const u32* s_minv, u64 R, u64 wb,
+                                         u32 I) {
+  const PrimeRec pr = e.recs[I];
+  u32 x = xq[I] + fk_bmod(R, pr.q, pr.magic);
+  x = min(x, x - pr.q);
+  const u32 s = fk_mulmod(x, s_minv[I], pr.q, pr.magic);
+  const u32 t = s + fk_bmod(wb, pr.q, pr.magic);
+  return min(t, t - pr.q);
+}
 
 struct SieveArgs {
   const DevEngine* engines;
@@ -461,7 +490,20 @@ __device__ __forceinline__ void sieve_block(
   S.chain_R[tid] = R;
   S.chain_w0[tid] = w0;
   u32 rho[NS];
-  Pat<P0, 0, NS>::setup(rho, R, 64ull * w0, a.xq + it.xq_off, S.minv);
+  if (G == 32) {
+    // the whole warp sweeps one lane: thread I works out prime I's base
+    // index once and the warp shares it (instead of every thread
+    // computing all NS of them)
+    const u32* __restrict__ xqi = a.xq + it.xq_off;
+    const u64 wb = chunk * 32ull * it.Tc;
+    u32 b0 = 0, b1 = 0;
+    if (wl < (u32)NS) b0 = lane_base(e, xqi, S.minv, R, wb, wl);
+    if (NS > 32 && wl + 32 < (u32)NS)
+      b1 = lane_base(e, xqi, S.minv, R, wb, wl + 32);
+    Pat<P0, 0, NS>::spread(rho, b0, b1, wl);
+  } else {
+    Pat<P0, 0, NS>::setup(rho, R, 64ull * w0, a.xq + it.xq_off, S.minv);
+  }
   u32 qn = 0;
   if (active) {
     // the chain's words in range: j < Tc with w0 + j*stride < ceil(U/64)
