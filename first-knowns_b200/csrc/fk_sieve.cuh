@@ -156,18 +156,20 @@ struct Pat {
     k[I] = (u32)(((u32)(u0 % q) * i64 + s) % q);
     Pat<P0, I + 1, NS>::setup(k, R, u0, xq, s_minv);
   }
-  // The table indexes of a warp sweeping one lane, thread wl from word
-  // base + wl: (base_I + wl) mod q, base_I held by thread I (b0) or, for
-  // I >= 32, by thread I - 32 (b1).
-  static __device__ __forceinline__ void spread(u32* k, u32 b0, u32 b1,
-                                                u32 wl) {
+  // The table indexes of a group of GW threads sweeping one lane, thread
+  // t of the group from word base + t: (base_I + t) mod q, base_I held in
+  // v[I / GW] by thread I mod GW of the group.
+  template <int GW>
+  static __device__ __forceinline__ void spread(u32* k, const u32* v,
+                                                u32 t) {
     constexpr u32 q = fk_nth_prime(P0 + I);
-    const u32 b = __shfl_sync(0xffffffffu, I < 32 ? b0 : b1, I & 31);
-    // wl < 32: below q from the 37 up; the 17 ... 31 of the 13# and 17#
-    // families reduce it first, so one subtraction still ends in [0, q)
-    const u32 r = b + (q > 31 ? wl : wl % q);
+    const u32 b = __shfl_sync(0xffffffffu, v[I / GW], I % GW, GW);
+    // t < GW: below q for every prime when GW = 8 and from the 37 up when
+    // GW = 32; the 17 ... 31 of the 13# and 17# families reduce it first,
+    // so one subtraction still ends in [0, q)
+    const u32 r = b + (q >= (u32)GW ? t : t % q);
     k[I] = min(r, r - q);
-    Pat<P0, I + 1, NS>::spread(k, b0, b1, wl);
+    Pat<P0, I + 1, NS>::template spread<GW>(k, v, t);
   }
 };
 template <int P0, int NS>
@@ -176,7 +178,8 @@ struct Pat<P0, NS, NS> {
   static __device__ __forceinline__ void word2(const u64*, u32*, u64*) {}
   static __device__ __forceinline__ void setup(u32*, u64, u64, const u32*,
                                                const u32*) {}
-  static __device__ __forceinline__ void spread(u32*, u32, u32, u32) {}
+  template <int GW>
+  static __device__ __forceinline__ void spread(u32*, const u32*, u32) {}
 };
 
 // Pattern prime I's table index at word wb of lane R: (wb + s) mod q with
@@ -192,6 +195,24 @@ __device__ __forceinline__ u32 lane_base(const DevEngine& e,
   const u32 s = fk_mulmod(x, s_minv[I], pr.q, pr.magic);
   const u32 t = s + fk_bmod(wb, pr.q, pr.magic);
   return min(t, t - pr.q);
+}
+
+// The table indexes of a group of GW threads sweeping one lane from word
+// wb, thread t at word wb + t: thread t computes the base index of the
+// pattern primes t, t + GW, ... and the group shares them by shuffle.
+template <int P0, int NS, int GW>
+__device__ __forceinline__ void shared_setup(u32* rho, const DevEngine& e,
+                                             const u32* __restrict__ xq,
+                                             const u32* s_minv, u64 R,
+                                             u64 wb, u32 t) {
+  constexpr int K = (NS + GW - 1) / GW;
+  u32 v[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    const u32 I = t + (u32)(j * GW);
+    v[j] = I < (u32)NS ? lane_base(e, xq, s_minv, R, wb, I) : 0u;
+  }
+  Pat<P0, 0, NS>::template spread<GW>(rho, v, t);
 }
 
 struct SieveArgs {
@@ -494,13 +515,12 @@ __device__ __forceinline__ void sieve_block(
     // the whole warp sweeps one lane: thread I works out prime I's base
     // index once and the warp shares it (instead of every thread
     // computing all NS of them)
-    const u32* __restrict__ xqi = a.xq + it.xq_off;
-    const u64 wb = chunk * 32ull * it.Tc;
-    u32 b0 = 0, b1 = 0;
-    if (wl < (u32)NS) b0 = lane_base(e, xqi, S.minv, R, wb, wl);
-    if (NS > 32 && wl + 32 < (u32)NS)
-      b1 = lane_base(e, xqi, S.minv, R, wb, wl + 32);
-    Pat<P0, 0, NS>::spread(rho, b0, b1, wl);
+    shared_setup<P0, NS, 32>(rho, e, a.xq + it.xq_off, S.minv, R,
+                             chunk * 32ull * it.Tc, wl);
+  } else if (G == 8) {
+    // the same within each group of eight threads sweeping one lane
+    shared_setup<P0, NS, 8>(rho, e, a.xq + it.xq_off, S.minv, R,
+                            chunk * 8ull * it.Tc, wl & 7u);
   } else {
     Pat<P0, 0, NS>::setup(rho, R, 64ull * w0, a.xq + it.xq_off, S.minv);
   }
