@@ -1,5 +1,5 @@
-// fk_sieve_k.cu -- the pattern-sieve kernel variants k_sieve<P0, NS> and
-// the dispatch of every sieve launch (fk_launch.h).
+// fk_sieve_k.cu -- the pattern-sieve kernel variants k_sieve<P0, NS, DYN>
+// and the dispatch of every sieve launch (fk_launch.h).
 #include "fk_launch.h"
 
 namespace fk {
